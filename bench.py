@@ -1,0 +1,435 @@
+"""Benchmark of the SSAM stencil path on B200 (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ssam|reference]
+                    [--workload NAME]
+
+A step is one pass of the stencil over one grid.  The default workload is the
+memory-bound head of the 2D box family: 9-point box (radius 1), FP32,
+8192 x 8192, uniform[-1,1) input, coefficients uniform[0,1) normalised to
+sum 1, zero padding, one step per call.  Inputs are seeded synthetic data.
+
+Metric: GCells/s = cells x steps / time.  `value` is device-timed with the
+grid already in HBM (CUDA events on the launching stream, max over ranks);
+`e2e` is the same metric through the host-buffer C entry point
+(ssam_stencil2d_host) with the host<->device copies inside the timed region.
+Under torchrun every rank steps its own grid (independent shards, no
+collective on the data path: weak scaling).
+
+`--impl reference` times the reference's own CPU golden (`Convolution<T>`,
+ssai-2dconv/common.h:186-216, compiled from its sources into oracle/_ref) on
+the host cores for the same workload, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L2_BYTES = 126 * 1000 * 1000
+FALLBACK_HBM_GBS = 6650.0
+
+
+def workloads():
+    """name -> spec.  kind: 'box' / 'star' (ssam_stencil2d) or 'conv'."""
+    w = {}
+    for dt in ("f32", "f64", "bf16"):
+        for r in range(1, 6):
+            w[f"box{r}_{dt}_8192"] = dict(kind="box", r=r, dtype=dt, n=8192, steps=1,
+                                          boundary="zero")
+            w[f"box{r}_{dt}_8192_16steps"] = dict(kind="box", r=r, dtype=dt, n=8192,
+                                                  steps=16, boundary="zero")
+        for f in range(3, 22, 2):
+            w[f"conv{f}_{dt}_8192"] = dict(kind="conv", r=f // 2, f=f, dtype=dt, n=8192,
+                                           steps=1, boundary="zero")
+        for r in range(1, 7):
+            w[f"star{r}_{dt}_8192"] = dict(kind="star", r=r, dtype=dt, n=8192, steps=1,
+                                           boundary="zero")
+    w["star1_f32_4096_copy"] = dict(kind="star", r=1, dtype="f32", n=4096, steps=1,
+                                    boundary="copy", coeffs=[0.2] * 5)
+    return w
+
+
+DEFAULT = "box1_f32_8192"
+
+
+def taps(spec) -> int:
+    r = spec["r"]
+    if spec["kind"] == "star":
+        return 4 * r + 1
+    if spec["kind"] == "conv":
+        return spec["f"] ** 2
+    return (2 * r + 1) ** 2
+
+
+def coefficients(spec):
+    """Coefficients uniform[0,1) normalised to sum 1 (seeded)."""
+    if "coeffs" in spec:
+        return spec["coeffs"]
+    g = np.random.Generator(np.random.PCG64(1234 + spec["r"]))
+    c = g.random(taps(spec))
+    return list(c / c.sum())
+
+
+def np_dtype(dt):
+    return {"f32": np.float32, "f64": np.float64}.get(dt)
+
+
+def elem_size(dt) -> int:
+    return {"f32": 4, "f64": 8, "bf16": 2}[dt]
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def load_traffic(name):
+    """dram__bytes_read.sum + dram__bytes_write.sum per launch from the
+    committed ncu summary (profiles/traffic.json), if one covers the
+    workload."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f).get(name)
+    except Exception:
+        return None
+
+
+# ----------------------------------------------------------- clock sampler --
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "50"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        time.sleep(0.15)
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.1)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------- CPU timing --
+
+def cpu_reference_rate(spec, budget_s: float, seed: int = 7):
+    """The reference's compiled Convolution<T> on the host cores: returns
+    (GCells/s, sample description, cores).  Runs whole grids until
+    ~budget_s, or a row slab of the grid when one grid takes longer."""
+    import oracle
+    if not oracle.have_ref():
+        raise RuntimeError("oracle/_ref is not built")
+    dt = np_dtype(spec["dtype"]) or np.float32
+    n = spec["n"]
+    g = np.random.Generator(np.random.PCG64(seed))
+    c = coefficients(spec)
+    if spec["kind"] == "star":
+        r = spec["r"]
+        m = np.zeros((2 * r + 1, 2 * r + 1))
+        m[r, r] = c[0]
+        for k in range(1, r + 1):
+            m[r - k, r], m[r + k, r], m[r, r - k], m[r, r + k] = c[1 + 4 * (k - 1): 5 + 4 * (k - 1)]
+    else:
+        f = 2 * spec["r"] + 1 if spec["kind"] == "box" else spec["f"]
+        m = np.array(c).reshape(f, f)
+    m = m.astype(dt)
+    # probe on a slab to size the sample
+    rows = min(n, 256)
+    slab = g.uniform(-1, 1, size=(rows, n)).astype(dt)
+    t0 = time.perf_counter()
+    oracle.ref_convolution(slab, m)
+    per_row = (time.perf_counter() - t0) / rows
+    steps = spec["steps"]
+    per_grid = per_row * n * steps
+    if per_grid <= budget_s:
+        src = g.uniform(-1, 1, size=(n, n)).astype(dt)
+        reps = max(1, int(budget_s / per_grid))
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            cur = src
+            for _ in range(steps):
+                cur = oracle.ref_convolution(cur, m)
+        el = time.perf_counter() - t0
+        cells = reps * n * n * steps
+        sample = f"{reps} x full {n}x{n} grid x {steps} step(s)"
+    else:
+        rows = max(2 * spec["r"] + 1, min(n, int(budget_s / (per_row * steps))))
+        src = g.uniform(-1, 1, size=(rows, n)).astype(dt)
+        t0 = time.perf_counter()
+        cur = src
+        for _ in range(steps):
+            cur = oracle.ref_convolution(cur, m)
+        el = time.perf_counter() - t0
+        cells = rows * n * steps
+        sample = f"{rows}-row slab of the {n}x{n} grid x {steps} step(s)"
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    return cells / el / 1e9, sample, cores
+
+
+# ------------------------------------------------------------ reference arm --
+
+def run_reference(args, spec, name):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    n_steps = args.steps + args.warmup
+    budget = max(0.05, min(10.0, 150.0 / max(1, n_steps)))
+    rates = []
+    sample = cores = None
+    for i in range(n_steps):
+        rate, sample, cores = cpu_reference_rate(spec, budget, seed=i)
+        if i >= args.warmup:
+            rates.append(rate)
+    value = statistics.median(rates) if rates else None
+    cells = spec["n"] ** 2 * spec["steps"]
+    line = {
+        "impl": "reference", "metric": "GCells/s", "value": value, "unit": "GCells/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": (cells / (value * 1e9) * 1e3) if value else None,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": spec["dtype"], "data": "synthetic (seeded uniform[-1,1))",
+        "config": dict(workload=name, grid=f"{spec['n']}x{spec['n']}", kind=spec["kind"],
+                       radius=spec["r"], steps_per_call=spec["steps"],
+                       boundary=spec["boundary"]),
+        "cpu_baseline": {"value": value, "unit": "GCells/s", "cores": cores,
+                         "kind": "reference", "sample": f"per step: {sample}"},
+        "e2e": {"value": value, "unit": "GCells/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ our arm --
+
+def run_ssam(args, spec, name):
+    import torch
+    import torch.distributed as dist
+
+    import ssam_b200 as S
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+
+    n = spec["n"]
+    tdt = {"f32": torch.float32, "f64": torch.float64, "bf16": torch.bfloat16}[spec["dtype"]]
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1000 + rank)
+    srcs = [(torch.rand(n, n, device=dev, dtype=torch.float32, generator=gen) * 2 - 1).to(tdt)
+            for _ in range(2)]
+    dst = torch.empty_like(srcs[0])
+    c = coefficients(spec)
+    r = spec["r"]
+    kind = spec["kind"]
+    shape = S.STAR if kind == "star" else S.BOX
+    stream = torch.cuda.current_stream(dev)
+
+    if kind == "conv":
+        w = np.array(c).reshape(spec["f"], spec["f"])
+
+        def step(i):
+            S.conv2d(srcs[i % 2], w, boundary=spec["boundary"], dst=dst, stream=stream)
+    else:
+        def step(i):
+            S.stencil2d(srcs[i % 2], c, r, shape, steps=spec["steps"],
+                        boundary=spec["boundary"], dst=dst, stream=stream)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    launches0 = S.lib().ssam_kernel_launches()
+    t_start.record(stream)
+    for i in range(args.steps):
+        ev[i][0].record(stream)
+        step(i)
+        ev[i][1].record(stream)
+    t_end.record(stream)
+    launches = S.lib().ssam_kernel_launches() - launches0
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    total_ms = t_start.elapsed_time(t_end)
+    launch_ms = [a.elapsed_time(b) for a, b in ev]
+    avg_launch_ms = sum(launch_ms) / len(launch_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = t.item()
+
+    cells = n * n * spec["steps"]
+    value = cells * args.steps * world / (total_ms / 1e3) / 1e9
+    es = elem_size(spec["dtype"])
+    # launches per call: one per chained temporal block (counted by the library)
+    launches_per_step = max(1, launches // args.steps)
+    peak, peak_kind = load_peaks()
+    # algorithmic bytes of one call: read + write each cell once per launch
+    alg_bytes = 2 * n * n * es * launches_per_step
+    achieved = alg_bytes / (avg_launch_ms / 1e3) / 1e9
+    traffic = load_traffic(name)
+
+    # end to end: host buffers through ssam_stencil2d_host, copies timed
+    e2e = None
+    if kind != "conv":
+        k_e2e = max(3, min(args.steps, 20))
+        hs = srcs[0].cpu().pin_memory()
+        hd = torch.empty_like(hs).pin_memory()
+        for _ in range(2):
+            S.stencil2d_host(hs, hd, c, r, shape, spec["steps"], spec["boundary"], dev, stream)
+        torch.cuda.synchronize()
+        barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(k_e2e):
+            S.stencil2d_host(hs, hd, c, r, shape, spec["steps"], spec["boundary"], dev, stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        e_ms = a.elapsed_time(b)
+        if world > 1:
+            t = torch.tensor([e_ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_ms = t.item()
+        e2e = {"value": cells * k_e2e * world / (e_ms / 1e3) / 1e9, "unit": "GCells/s",
+               "h2d_bytes_per_step": n * n * es, "d2h_bytes_per_step": n * n * es,
+               "steps": k_e2e}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            rate, sample, cores = cpu_reference_rate(spec, budget_s=10.0)
+            cpu = {"value": rate, "unit": "GCells/s", "cores": cores, "kind": "reference",
+                   "sample": sample}
+        except Exception as exc:  # the GPU number stands without it
+            cpu = {"value": None, "unit": "GCells/s", "cores": None, "kind": "reference",
+                   "sample": f"unavailable: {exc}"}
+
+    if rank == 0:
+        line = {
+            "metric": "GCells/s", "value": value, "unit": "GCells/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": spec["dtype"],
+            "data": "synthetic (seeded uniform[-1,1), coefficients uniform[0,1) normalised)",
+            "config": {"workload": name, "grid": f"{n}x{n}", "kind": kind, "radius": r,
+                       "taps": taps(spec), "steps_per_call": spec["steps"],
+                       "boundary": spec["boundary"],
+                       "l2": "inputs larger than L2: two alternating "
+                             f"{n * n * es / 2**20:.0f} MiB inputs + output vs 126 MB L2",
+                       "parallelism": f"dp{world} (independent grid per GPU)"},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": peak_kind,
+                         "traffic": traffic,
+                         "algorithmic_bytes_per_launch": alg_bytes / launches_per_step},
+            "clocks": clk,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ssam", choices=["ssam", "reference"])
+    ap.add_argument("--workload", default=DEFAULT)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    wl = workloads()
+    if args.workload not in wl:
+        raise SystemExit(f"unknown workload {args.workload}; known: {sorted(wl)}")
+    spec = wl[args.workload]
+    if args.impl == "reference":
+        run_reference(args, spec, args.workload)
+    else:
+        run_ssam(args, spec, args.workload)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,174 @@
+/*
+ * ssam.h -- C ABI of the B200-native register-cache systolic stencil and
+ * convolution library (libssam_b200.so).
+ *
+ * Conventions shared by every entry point
+ * ---------------------------------------
+ *  - Grids are row-major with x fastest, exactly as the reference lays them
+ *    out: 2D index = pitch*y + x (ssai-2dstencil/stencil2D_5pt-v1.cu:29,
+ *    ssai-2dconv/conv2D.cu:32), 3D index = nx*ny*z + nx*y + x
+ *    (ssai-3dstencil/tmp3d7pt-v2.cu:107).  `pitch` is counted in ELEMENTS, like
+ *    the reference's `widthStride` (conv2D.cu:11).
+ *  - All grid pointers are DEVICE pointers owned by the caller.  `src` is read
+ *    only; `dst` is a separate buffer (no in-place update), as in every
+ *    reference kernel (`const T* __restrict__ src, T* dst`).
+ *  - Calls are asynchronous on the caller's CUDA stream (`stream` is a
+ *    cudaStream_t; NULL = legacy default stream).  The reference is synchronous
+ *    on the default stream; callers that want that behaviour synchronise.
+ *  - Every function returns an ssam_status.  Nothing throws across the ABI.
+ *    ssam_last_error() returns a message for the calling thread's last failure.
+ *  - Coefficients are passed as HOST arrays of double and are converted once to
+ *    the compute type (float for F32/BF16/F16 storage, double for F64), the
+ *    same value the reference obtains from its `T`-typed literals.
+ *  - There is no CPU fallback: without a usable sm_100 device every compute
+ *    entry point fails with SSAM_ERR_CUDA.
+ */
+#ifndef SSAM_B200_H
+#define SSAM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SSAM_ABI_VERSION 1
+
+/* Exported symbols (the library is built with hidden visibility). */
+#if defined(__GNUC__)
+#define SSAM_API __attribute__((visibility("default")))
+#else
+#define SSAM_API
+#endif
+
+typedef enum ssam_status {
+  SSAM_OK = 0,
+  SSAM_ERR_INVALID = 1,     /* bad argument: null pointer, size, radius, pitch ... */
+  SSAM_ERR_UNSUPPORTED = 2, /* valid request that this build has no kernel for */
+  SSAM_ERR_CUDA = 3,        /* CUDA runtime error (launch, copy, no device) */
+  SSAM_ERR_NOMEM = 4,       /* device scratch allocation failed */
+  SSAM_ERR_TIMEOUT = 5      /* a bounded device-side wait gave up */
+} ssam_status;
+
+/* Storage type of the grid.  F32 and F64 compute in their own precision, as
+ * the reference does; BF16 and F16 are storage-only types that the kernels
+ * widen to float and accumulate in float. */
+typedef enum ssam_dtype {
+  SSAM_F32 = 0,
+  SSAM_F64 = 1,
+  SSAM_BF16 = 2,
+  SSAM_F16 = 3
+} ssam_dtype;
+
+/* What a tap that falls outside the grid reads, and what is written near the
+ * edge.
+ *  ZERO  : out-of-grid taps read 0 and every cell is computed -- the CPU golden
+ *          `Convolution` (ssai-2dconv/common.h:186-216) and the conv kernel
+ *          (conv2D.cu:36-41).
+ *  CLAMP : out-of-grid taps read the nearest edge cell and every cell is
+ *          computed -- the 2D/3D stencil kernels' halo load
+ *          (stencil2D_5pt-v1.cu:29-46, tmp3d7pt-v2.cu:107-121).  Single step
+ *          only.
+ *  COPY  : cells closer to the edge than the stencil reach keep their input
+ *          value every step (fixed / Dirichlet boundary); all other cells are
+ *          computed.  For 3D this is the reference gold with its output
+ *          initialised from the input (tmp3d7pt-v2.cu:278-298). */
+typedef enum ssam_boundary {
+  SSAM_BOUNDARY_ZERO = 0,
+  SSAM_BOUNDARY_CLAMP = 1,
+  SSAM_BOUNDARY_COPY = 2
+} ssam_boundary;
+
+/* Tap pattern of a square 2D stencil of radius r. */
+typedef enum ssam_shape2d {
+  /* (2r+1)x(2r+1) matrix, non-zero only on the centre row and column: the
+   * reference's 5/9/13/17/21/25-pt star stencils (stencil2D_25pt.cu:167-181). */
+  SSAM_STAR = 0,
+  /* full (2r+1)x(2r+1) box: 9/25/49/81/121-pt (stencil2D_81pt.cu,
+   * stencil2D_121pt.cu) and the 64-pt 9x9 with a zero centre cross
+   * (stencil2D_64pt.cu:255-266). */
+  SSAM_BOX = 1
+} ssam_shape2d;
+
+/* ---------------------------------------------------------------- library */
+
+/* Message for the calling thread's most recent non-OK status ("" if none). */
+SSAM_API const char* ssam_last_error(void);
+
+/* SSAM_ABI_VERSION of the loaded library. */
+SSAM_API int ssam_abi_version(void);
+
+/* Number of kernels this library has launched in the process so far (all
+ * threads, all devices); lets a caller count the launches of a region. */
+SSAM_API uint64_t ssam_kernel_launches(void);
+
+/* Device scratch (multi-step ping-pong grids, host-call staging) comes from a
+ * library memory pool per device that keeps freed memory mapped for the next
+ * call.  This returns all of it that is not in use to the driver. */
+SSAM_API int ssam_trim_scratch(void);
+
+/* ------------------------------------------------------------ 2D stencils */
+
+/*
+ * One or more time steps of a square 2D stencil of radius r (1..10).
+ *
+ * Replaces the reference kernels and their host drivers
+ *   stencil2d_v1::j2d5pt          ssai-2dstencil/stencil2D_5pt-v1.cu:8-129
+ *   j2d9pt .. j2d25pt (star r=2..6)  stencil2D_9pt.cu:9-87 .. stencil2D_25pt.cu:9-126
+ *   j2d64pt / j2d81pt / j2d121pt(+v2/v3/v4)  stencil2D_64pt.cu:73-214,
+ *                                 stencil2D_81pt.cu:91-249, stencil2D_121pt.cu:131-331
+ *   stencil2d_tmp::j2d5pt / j2d9pt (ITERATIVE_COUNT fused steps)
+ *                                 stencil2d_temp_5pt.cu:9-82, stencil2d_temp_9pt.cu:13-95
+ * and the entry points `int stencil_<N>pt_<float|double>(argc, argv)` and
+ * `stencil_tmp_<N>pt_*` that drive them (ssai-2dstencil/main.cpp:29-53).
+ *
+ * coeffs:
+ *   SSAM_STAR: 4r+1 values in the reference's kernel-argument order:
+ *              c, then for ring k=1..r: n_k, s_k, w_k, e_k
+ *              (stencil2D_25pt.cu:10-16: fc, fn0, fs0, fw0, fe0, fn1, ...).
+ *              n = row y-k, s = row y+k, w = column x-k, e = column x+k.
+ *   SSAM_BOX : (2r+1)^2 values, row-major, coeffs[(dy+r)*(2r+1) + (dx+r)]
+ *              weights in(y+dy, x+dx) -- the reference's `_F<row><col>`
+ *              tables (stencil2D_81pt.cu:4-84).
+ * steps >= 1: time steps; step k+1 reads step k's result.  Steps are fused in
+ * registers (temporal blocking) and chained through a device scratch grid that
+ * the library allocates stream-ordered when more than one launch is needed.
+ * CLAMP is single-step only.
+ */
+SSAM_API int ssam_stencil2d(const void* src, void* dst, int64_t width, int64_t height,
+                   int64_t pitch, int dtype, int shape, int radius,
+                   const double* coeffs, int steps, int boundary, void* stream);
+
+/*
+ * ssam_stencil2d on HOST buffers: the grid is copied to the device, stepped
+ * and copied back, like the reference Test() drivers (DevBuffer::CopyFromHost
+ * -> kernel -> CopyToHost, stencil2D_5pt-v1.cu:164-203).  Device memory is
+ * allocated stream-ordered inside the call.  A single step is pipelined over
+ * row bands (upload, compute and download overlap).  Returns once the work is
+ * queued on `stream`; h_dst is valid after the stream is synchronised.  Use
+ * page-locked host memory for full copy bandwidth.
+ */
+SSAM_API int ssam_stencil2d_host(const void* h_src, void* h_dst, int64_t width,
+                                 int64_t height, int64_t pitch, int dtype, int shape,
+                                 int radius, const double* coeffs, int steps,
+                                 int boundary, void* stream);
+
+/*
+ * Generic 2D correlation with an fw x fh weight matrix (1 <= fw, fh <= 28):
+ *   dst(y, x) = sum_{n<fh, m<fw} weight[n*fw + m] * src(y + n - fh/2, x + m - fw/2)
+ * Replaces CONV2D::kernel_convolution2D<T,B,P,FW,FH>
+ * (ssai-2dconv/conv2D.cu:9-70, weights `smem[n][m]` row n / column m) and its
+ * driver Test_conv2D / Test_2D (conv2D.cu:72-230).  The reference always zero
+ * pads (boundary = SSAM_BOUNDARY_ZERO); CLAMP and COPY are also accepted.
+ * Even and non-square filters follow the same offsets as the reference.
+ */
+SSAM_API int ssam_conv2d(const void* src, void* dst, int64_t width, int64_t pitch,
+                int64_t height, int dtype, const double* weight, int fw, int fh,
+                int boundary, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SSAM_B200_H */

@@ -1,0 +1,169 @@
+"""ssam_b200 -- B200-native register-cache systolic stencils and convolutions.
+
+Python front end over the C ABI of ``libssam_b200.so`` (``include/ssam.h``).
+It exists for tests, benchmarks and Python users; C/C++ callers link the
+shared library directly.  torch is used only to hold device memory and to
+name the CUDA stream -- every byte of compute runs in this package's own
+sm_100a kernels.  There is no CPU fallback: if the library is missing or no
+B200 is visible, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libssam_b200.so")
+
+OK, ERR_INVALID, ERR_UNSUPPORTED, ERR_CUDA, ERR_NOMEM, ERR_TIMEOUT = range(6)
+F32, F64, BF16, F16 = range(4)
+BOUNDARY = {"zero": 0, "clamp": 1, "copy": 2}
+STAR, BOX = 0, 1
+
+_STATUS_NAMES = {0: "SSAM_OK", 1: "SSAM_ERR_INVALID", 2: "SSAM_ERR_UNSUPPORTED",
+                 3: "SSAM_ERR_CUDA", 4: "SSAM_ERR_NOMEM", 5: "SSAM_ERR_TIMEOUT"}
+
+
+class SsamError(RuntimeError):
+    """A non-OK status from the C ABI; ``status`` holds the code."""
+
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{_STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+_i64 = ctypes.c_int64
+_int = ctypes.c_int
+_vp = ctypes.c_void_p
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def _declare(lib):
+    lib.ssam_last_error.restype = ctypes.c_char_p
+    lib.ssam_last_error.argtypes = []
+    lib.ssam_abi_version.restype = _int
+    lib.ssam_kernel_launches.restype = ctypes.c_uint64
+    lib.ssam_kernel_launches.argtypes = []
+    lib.ssam_stencil2d.restype = _int
+    lib.ssam_stencil2d.argtypes = [_vp, _vp, _i64, _i64, _i64, _int, _int, _int, _dp,
+                                   _int, _int, _vp]
+    lib.ssam_stencil2d_host.restype = _int
+    lib.ssam_stencil2d_host.argtypes = lib.ssam_stencil2d.argtypes
+    lib.ssam_conv2d.restype = _int
+    lib.ssam_conv2d.argtypes = [_vp, _vp, _i64, _i64, _i64, _int, _dp, _int, _int,
+                                _int, _vp]
+
+
+def lib():
+    """The loaded ``libssam_b200.so`` (ctypes)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is not built; run `python -m ssam_b200.build` "
+                "(there is no CPU fallback)")
+        _lib = ctypes.CDLL(LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+def _check(status: int) -> None:
+    if status != OK:
+        raise SsamError(status, lib().ssam_last_error().decode())
+
+
+def _dtype_code(t) -> int:
+    import torch
+    m = {torch.float32: F32, torch.float64: F64, torch.bfloat16: BF16, torch.float16: F16}
+    if t.dtype not in m:
+        raise TypeError(f"unsupported grid dtype {t.dtype}")
+    return m[t.dtype]
+
+
+def _doubles(vals):
+    vals = [float(v) for v in vals]
+    return (ctypes.c_double * len(vals))(*vals)
+
+
+def _stream_ptr(t, stream):
+    import torch
+    if stream is None:
+        stream = torch.cuda.current_stream(t.device)
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def _grid2d(src, dst):
+    import torch
+    if not src.is_cuda:
+        raise ValueError("src must be a CUDA tensor (use the *_host entry points for host buffers)")
+    if src.dim() != 2 or src.stride(1) != 1:
+        raise ValueError("2D grids must be row-major with unit x stride")
+    if dst is None:
+        dst = torch.empty_strided(src.shape, src.stride(), dtype=src.dtype, device=src.device)
+    if dst.shape != src.shape or dst.stride() != src.stride() or dst.dtype != src.dtype:
+        raise ValueError("dst must match src in shape, strides and dtype")
+    return dst
+
+
+def stencil2d(src, coeffs, radius: int, shape: int = STAR, steps: int = 1,
+              boundary: str = "zero", dst=None, stream=None):
+    """``steps`` steps of a square radius-``radius`` stencil (``ssam_stencil2d``).
+
+    ``coeffs``: STAR -> [c, n1, s1, w1, e1, n2, ...]; BOX -> (2r+1)^2 row-major.
+    """
+    dst = _grid2d(src, dst)
+    h, w = src.shape
+    c = _doubles(coeffs)
+    _check(lib().ssam_stencil2d(src.data_ptr(), dst.data_ptr(), w, h, src.stride(0),
+                                _dtype_code(src), shape, radius, c, steps,
+                                BOUNDARY[boundary], _stream_ptr(src, stream)))
+    return dst
+
+
+def stencil2d_host(src, dst, coeffs, radius: int, shape: int = STAR, steps: int = 1,
+                   boundary: str = "zero", device=None, stream=None):
+    """``ssam_stencil2d_host``: ``src``/``dst`` are CPU tensors (pinned for
+    full bandwidth); copies in, steps, copies out.  Queued on ``stream``;
+    synchronise before reading ``dst``."""
+    import torch
+    if src.is_cuda or dst.is_cuda:
+        raise ValueError("stencil2d_host takes host tensors")
+    if src.dim() != 2 or src.stride(1) != 1 or dst.shape != src.shape or \
+            dst.stride() != src.stride() or dst.dtype != src.dtype:
+        raise ValueError("src/dst must be matching row-major 2D host tensors")
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    if stream is None:
+        stream = torch.cuda.current_stream(dev)
+    h, w = src.shape
+    c = _doubles(coeffs)
+    with torch.cuda.device(dev):
+        _check(lib().ssam_stencil2d_host(src.data_ptr(), dst.data_ptr(), w, h, src.stride(0),
+                                         _dtype_code(src), shape, radius, c, steps,
+                                         BOUNDARY[boundary], ctypes.c_void_p(stream.cuda_stream)))
+    return dst
+
+
+def conv2d(src, weight, boundary: str = "zero", dst=None, stream=None):
+    """Correlation with an (fh, fw) weight matrix (``ssam_conv2d``)."""
+    dst = _grid2d(src, dst)
+    h, w = src.shape
+    rows = [list(map(float, r)) for r in (weight.tolist() if hasattr(weight, "tolist") else weight)]
+    fh, fw = len(rows), len(rows[0])
+    c = _doubles([v for r in rows for v in r])
+    _check(lib().ssam_conv2d(src.data_ptr(), dst.data_ptr(), w, src.stride(0), h,
+                             _dtype_code(src), c, fw, fh, BOUNDARY[boundary],
+                             _stream_ptr(src, stream)))
+    return dst
+
+
+def star_coeffs_from_matrix(m) -> list[float]:
+    """Reference kernel-argument order (stencil2D_25pt.cu:10-16) from a
+    (2r+1)x(2r+1) star matrix: c, then n_k, s_k, w_k, e_k for k = 1..r."""
+    rows = m.tolist() if hasattr(m, "tolist") else m
+    r = len(rows) // 2
+    out = [rows[r][r]]
+    for k in range(1, r + 1):
+        out += [rows[r - k][r], rows[r + k][r], rows[r][r - k], rows[r][r + k]]
+    return out

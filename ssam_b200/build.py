@@ -1,0 +1,163 @@
+"""In-tree build of libssam_b200.so for sm_100a.
+
+    python -m ssam_b200.build [-j N] [--ptxas-verbose]
+
+The kernel instantiation list below is the single source of truth for which
+(dtype, reach, shape, P, fused steps) kernels exist; the C ABI reports
+SSAM_ERR_UNSUPPORTED for anything else.  Generated instantiation units and
+objects go to ssam_b200/_build/ (not committed); the shared library lands
+next to this file so that it travels with the source tree.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import hashlib
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libssam_b200.so")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
+           "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr",
+           "-Wno-deprecated-gpu-targets"]
+
+# Hand-written (non-generated) translation units.
+SOURCES = ["api.cu", "autotune.cu"]
+
+DTYPES = {"f32": "float", "f64": "double", "bf16": "__nv_bfloat16", "f16": "__half"}
+
+
+def instances():
+    """(dtype, star, rl, rr, P, T) of every compiled 2D kernel."""
+    out = []
+    for dt in DTYPES:
+        wide = dt in ("f32", "f64")
+        # star r = 1..6 (5/9/13/17/21/25-pt)
+        for r in range(1, 7):
+            for p in (4, 8, 16):
+                out.append((dt, 1, r, r, p, 1))
+        # box r = 1..5 (9/25/49/81/121-pt; conv F = 3..11)
+        for r in range(1, 6):
+            for p in (4, 8, 16):
+                out.append((dt, 0, r, r, p, 1))
+        # temporal blocking for the bandwidth-bound radii
+        for star in (1, 0):
+            for r, ts in ((1, (2, 4, 8)), (2, (2, 4))):
+                for t in ts:
+                    out.append((dt, star, r, r, 8, t))
+        # every other square conv size up to 28 (even F has rl = rr + 1)
+        if wide:
+            for f in range(1, 29):
+                rl, rr = f // 2, f - 1 - f // 2
+                if f % 2 == 1 and 1 <= rl <= 5:
+                    continue
+                out.append((dt, 0, rl, rr, 4, 1))
+    return out
+
+
+def _gen_units(chunk: int = 6):
+    os.makedirs(os.path.join(BUILD, "gen"), exist_ok=True)
+    by_dt: dict[str, list] = {}
+    for inst in instances():
+        by_dt.setdefault(inst[0], []).append(inst)
+    units = []
+    for dt, lst in by_dt.items():
+        for c in range(0, len(lst), chunk):
+            part = lst[c:c + chunk]
+            name = f"inst2d_{dt}_{c // chunk:02d}.cu"
+            lines = ["// generated by ssam_b200/build.py -- do not edit",
+                     '#include "../../csrc/stencil2d.cuh"', "namespace ssam {"]
+            for (_, star, rl, rr, p, t) in part:
+                tag = f"{'s' if star else 'b'}_{rl}_{rr}_{p}_{t}"
+                lines.append(
+                    f"static Register2D<{DTYPES[dt]}, {rl}, {rr}, {rl}, {rr}, "
+                    f"{'true' if star else 'false'}, {p}, {t}> reg_{tag};")
+            lines.append("}  // namespace ssam")
+            text = "\n".join(lines) + "\n"
+            path = os.path.join(BUILD, "gen", name)
+            if not os.path.exists(path) or open(path).read() != text:
+                with open(path, "w") as f:
+                    f.write(text)
+            units.append(path)
+    return units
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _headers_digest() -> str:
+    h = hashlib.sha1()
+    for root in (CSRC, os.path.join(os.path.dirname(HERE), "include")):
+        for name in sorted(os.listdir(root)):
+            if name.endswith((".cuh", ".h")):
+                with open(os.path.join(root, name), "rb") as f:
+                    h.update(f.read())
+    h.update(" ".join(NVFLAGS + ARCH).encode())
+    return h.hexdigest()
+
+
+def _compile(src: str, obj: str, extra: list[str], stamp: str) -> str:
+    stamp_path = obj + ".stamp"
+    if (os.path.exists(obj) and os.path.exists(stamp_path)
+            and open(stamp_path).read() == stamp
+            and os.path.getmtime(obj) >= os.path.getmtime(src)):
+        return obj
+    cmd = [_nvcc(), *ARCH, *NVFLAGS, *extra, "-c", src, "-o", obj]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed on {src}:\n{r.stdout}\n{r.stderr}")
+    if r.stderr.strip() and "-Xptxas" in " ".join(extra):
+        with open(obj + ".ptxas.txt", "w") as f:
+            f.write(r.stderr)
+    with open(stamp_path, "w") as f:
+        f.write(stamp)
+    return obj
+
+
+def build(jobs: int | None = None, ptxas_verbose: bool = False, quiet: bool = True) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    units = [os.path.join(CSRC, s) for s in SOURCES] + _gen_units()
+    extra = ["-Xptxas", "-v"] if ptxas_verbose else []
+    stamp = _headers_digest() + ("v" if ptxas_verbose else "")
+    jobs = jobs or max(1, os.cpu_count() or 1)
+    objs = []
+    with cf.ThreadPoolExecutor(jobs) as ex:
+        futs = []
+        for u in units:
+            obj = os.path.join(BUILD, os.path.basename(u).replace(".cu", ".o"))
+            futs.append(ex.submit(_compile, u, obj, extra, stamp))
+        for f in futs:
+            objs.append(f.result())
+    tmp = LIB + ".tmp"
+    cmd = [_nvcc(), *ARCH, "-shared", "-o", tmp, *objs, "-cudart", "static",
+           "-Xlinker", "--exclude-libs,ALL"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    os.replace(tmp, LIB)
+    if not quiet:
+        print(f"built {LIB} from {len(objs)} units")
+    return LIB
+
+
+def main(argv=None) -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("-j", "--jobs", type=int, default=None)
+    ap.add_argument("--ptxas-verbose", action="store_true")
+    a = ap.parse_args(argv)
+    build(a.jobs, a.ptxas_verbose, quiet=False)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,24 @@
+// Launch-parameter choice for the 2D kernels: built-in defaults, plus a
+// cache of measured choices filled by the autotuner (ssam_autotune_* in the C
+// ABI) and optionally persisted to a text file.
+#pragma once
+
+#include <stdint.h>
+
+namespace ssam {
+
+struct TuneChoice {
+  int p;      // output rows per thread (template P)
+  int warps;  // warps per block
+};
+
+// Measured choice for this stencil, fused depth and grid size, if any.
+bool tune_lookup_2d(int dtype, int rl, int rr, int rt, int rb, int star, int t,
+                    int64_t w, int64_t h, TuneChoice* out);
+// Static choice used when nothing was measured.
+TuneChoice tune_default_2d(int dtype, int rl, int rr, int rt, int rb, int star, int t);
+// Largest number of steps to fuse in one launch for a `steps`-step run.
+int tune_depth_2d(int dtype, int rl, int rr, int rt, int rb, int star, int64_t w,
+                  int64_t h, int steps);
+
+}  // namespace ssam

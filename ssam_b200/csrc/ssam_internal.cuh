@@ -1,0 +1,148 @@
+// Internal declarations shared by the CUDA translation units of
+// libssam_b200.so: status plumbing, storage-type traits, 128-bit row
+// loads/stores, and the kernel registry that the C ABI dispatches through.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/ssam.h"
+
+namespace ssam {
+
+// ------------------------------------------------------------------ status --
+
+// Records `msg` as the calling thread's last error and returns `st`.
+int fail(int st, const std::string& msg);
+// Maps a CUDA error to SSAM_ERR_CUDA with the runtime's message.
+int fail_cuda(cudaError_t e, const char* what);
+
+// Process-wide count of kernel launches (ssam_kernel_launches).
+void count_launch();
+
+// Stream-ordered device scratch from the library's per-device pool.
+int scratch_alloc(void** p, size_t bytes, cudaStream_t s);
+void scratch_free(void* p, cudaStream_t s);
+
+#define SSAM_CUDA_TRY(expr)                                \
+  do {                                                       \
+    cudaError_t _e = (expr);                                 \
+    if (_e != cudaSuccess) return ::ssam::fail_cuda(_e, #expr); \
+  } while (0)
+
+// ------------------------------------------------------------ dtype traits --
+
+// TA = accumulation type, V = elements a thread owns along x (one or two
+// 16-byte chunks).
+template <typename TS> struct Traits;
+template <> struct Traits<float> {
+  using TA = float;
+  static constexpr int V = 4;
+  static constexpr int DT = SSAM_F32;
+};
+template <> struct Traits<double> {
+  using TA = double;
+  static constexpr int V = 4;
+  static constexpr int DT = SSAM_F64;
+};
+template <> struct Traits<__nv_bfloat16> {
+  using TA = float;
+  static constexpr int V = 8;
+  static constexpr int DT = SSAM_BF16;
+};
+template <> struct Traits<__half> {
+  using TA = float;
+  static constexpr int V = 8;
+  static constexpr int DT = SSAM_F16;
+};
+
+inline size_t dtype_size(int dt) {
+  return dt == SSAM_F64 ? 8 : (dt == SSAM_F32 ? 4 : 2);
+}
+
+__device__ __forceinline__ float to_acc(float v) { return v; }
+__device__ __forceinline__ double to_acc(double v) { return v; }
+__device__ __forceinline__ float to_acc(__nv_bfloat16 v) { return __bfloat162float(v); }
+__device__ __forceinline__ float to_acc(__half v) { return __half2float(v); }
+
+template <typename TS> __device__ __forceinline__ TS from_acc(float v);
+template <> __device__ __forceinline__ float from_acc<float>(float v) { return v; }
+template <> __device__ __forceinline__ __nv_bfloat16 from_acc<__nv_bfloat16>(float v) {
+  return __float2bfloat16_rn(v);
+}
+template <> __device__ __forceinline__ __half from_acc<__half>(float v) {
+  return __float2half_rn(v);
+}
+template <typename TS> __device__ __forceinline__ TS from_acc(double v);
+template <> __device__ __forceinline__ double from_acc<double>(double v) { return v; }
+
+// V consecutive elements starting at a 16-byte aligned address, as 16-byte
+// (128-bit) transactions.
+template <typename TS, int V, typename TA>
+__device__ __forceinline__ void load_vec(TA (&r)[V], const TS* __restrict__ p) {
+  static_assert((V * sizeof(TS)) % 16 == 0, "whole 16-byte chunks");
+  constexpr int CH = V * sizeof(TS) / 16;
+  constexpr int PER = 16 / sizeof(TS);
+#pragma unroll
+  for (int c = 0; c < CH; ++c) {
+    const uint4 u = __ldg(reinterpret_cast<const uint4*>(p) + c);
+    const TS* e = reinterpret_cast<const TS*>(&u);
+#pragma unroll
+    for (int k = 0; k < PER; ++k) r[c * PER + k] = to_acc(e[k]);
+  }
+}
+
+template <typename TS, int V, typename TA>
+__device__ __forceinline__ void store_vec(TS* __restrict__ p, const TA (&r)[V]) {
+  constexpr int CH = V * sizeof(TS) / 16;
+  constexpr int PER = 16 / sizeof(TS);
+#pragma unroll
+  for (int c = 0; c < CH; ++c) {
+    uint4 u;
+    TS* e = reinterpret_cast<TS*>(&u);
+#pragma unroll
+    for (int k = 0; k < PER; ++k) e[k] = from_acc<TS>(r[c * PER + k]);
+    reinterpret_cast<uint4*>(p)[c] = u;
+  }
+}
+
+// ---------------------------------------------------------- kernel registry --
+
+// One compiled 2D stencil kernel: radii left/right/top/bottom, tap pattern,
+// outputs per thread along y (P) and fused time steps (T).
+struct Key2D {
+  int dtype, rl, rr, rt, rb, star, p, t;
+  bool operator<(const Key2D& o) const;
+  bool operator==(const Key2D& o) const;
+};
+
+struct Launch2D {
+  const void* src;
+  void* dst;
+  int64_t width, height, pitch;
+  int64_t y_begin, y_end;  // rows of the grid this launch writes
+  int boundary;
+  const double* coef;  // (rt+rb+1) x (rl+rr+1) row-major, host
+  int warps_per_block;
+  cudaStream_t stream;
+};
+
+using LaunchFn2D = cudaError_t (*)(const Launch2D&);
+
+struct Kernel2DInfo {
+  LaunchFn2D launch;
+  const void* func;  // the __global__ symbol, for occupancy queries
+  int vec;           // elements per thread along x
+};
+
+void register_2d(const Key2D& k, const Kernel2DInfo& info);
+const Kernel2DInfo* find_2d(const Key2D& k);
+// All registered kernels matching dtype/radii/shape (any P, T).
+void list_2d(int dtype, int rl, int rr, int rt, int rb, int star,
+             void (*cb)(const Key2D&, const Kernel2DInfo&, void*), void* user);
+
+}  // namespace ssam

@@ -1,0 +1,71 @@
+"""The C ABI library loads on a machine without a GPU, exports every entry
+point that include/ssam.h declares, and rejects bad arguments before it
+touches CUDA (no compute is launched here)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+import ssam_b200 as S
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                      "include", "ssam.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return re.findall(r"SSAM_API\s+[\w\s\*]+?\b(ssam_\w+)\s*\(", text)
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "ssam_stencil2d" in names and "ssam_conv2d" in names
+    assert len(names) == len(set(names))
+
+
+@pytest.mark.parametrize("name", declared_functions())
+def test_library_exports_declared_symbol(name):
+    lib = ctypes.CDLL(S.LIB_PATH)
+    assert hasattr(lib, name), f"{name} declared in include/ssam.h but not exported"
+
+
+def test_abi_version():
+    assert S.lib().ssam_abi_version() == 1
+
+
+FAKE_SRC = 0x7f0000000000
+FAKE_DST = 0x7f1000000000
+
+
+def _st2d(**kw):
+    a = dict(src=FAKE_SRC, dst=FAKE_DST, w=64, h=64, pitch=64, dtype=S.F32, shape=S.STAR,
+             r=1, coeffs=[0.2] * 5, steps=1, bnd=0)
+    a.update(kw)
+    c = (ctypes.c_double * max(1, len(a["coeffs"])))(*a["coeffs"]) if a["coeffs"] is not None else None
+    return S.lib().ssam_stencil2d(a["src"], a["dst"], a["w"], a["h"], a["pitch"], a["dtype"],
+                                  a["shape"], a["r"], c, a["steps"], a["bnd"], None)
+
+
+@pytest.mark.parametrize("kw", [
+    dict(src=0), dict(dst=0), dict(w=0), dict(h=-1), dict(pitch=10), dict(dtype=9),
+    dict(shape=7), dict(r=0), dict(r=7), dict(shape=S.BOX, r=11), dict(coeffs=None),
+    dict(steps=0), dict(bnd=5), dict(bnd=1, steps=2), dict(dst=FAKE_SRC + 128),
+])
+def test_stencil2d_rejects_bad_arguments(kw):
+    assert _st2d(**kw) == S.ERR_INVALID
+    assert S.lib().ssam_last_error().decode()
+
+
+@pytest.mark.parametrize("fw,fh", [(0, 3), (3, 0), (29, 3), (3, 29)])
+def test_conv2d_rejects_bad_filter(fw, fh):
+    w = (ctypes.c_double * 9)(*([1.0] * 9))
+    st = S.lib().ssam_conv2d(FAKE_SRC, FAKE_DST, 64, 64, 64, S.F32, w, fw, fh, 0, None)
+    assert st == S.ERR_INVALID
+
+
+def test_python_front_end_refuses_host_tensors():
+    import torch
+    with pytest.raises(ValueError):
+        S.stencil2d(torch.zeros(8, 8), [0.2] * 5, 1)
