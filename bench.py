@@ -56,6 +56,13 @@ def workloads():
                                            boundary="zero")
     w["star1_f32_4096_copy"] = dict(kind="star", r=1, dtype="f32", n=4096, steps=1,
                                     boundary="copy", coeffs=[0.2] * 5)
+    # 3D, 512^3, 100 steps per call (one captured CUDA graph), fixed boundary
+    for dt in ("f32", "bf16", "f64"):
+        for gold, r in (("j3d7pt", 1), ("j3d13pt", 2), ("poisson", 1)):
+            w[f"{gold}_{dt}_512_100steps"] = dict(kind="3d", gold=gold, r=r, dtype=dt, n=512,
+                                                  steps=100, boundary="copy")
+            w[f"{gold}_{dt}_512"] = dict(kind="3d", gold=gold, r=r, dtype=dt, n=512,
+                                         steps=1, boundary="copy")
     return w
 
 
@@ -64,6 +71,8 @@ DEFAULT = "box1_f32_8192"
 
 def taps(spec) -> int:
     r = spec["r"]
+    if spec["kind"] == "3d":
+        return {"j3d7pt": 7, "j3d13pt": 13, "poisson": 19}[spec["gold"]]
     if spec["kind"] == "star":
         return 4 * r + 1
     if spec["kind"] == "conv":
@@ -71,10 +80,25 @@ def taps(spec) -> int:
     return (2 * r + 1) ** 2
 
 
+def cube3d(spec) -> np.ndarray:
+    """The reference's own 3D coefficients (_F<z><y><x> defines, read from the
+    committed tests/golden/coefficients.json), scaled to sum 1 so that 100
+    steps stay bounded."""
+    with open(os.path.join(ROOT, "tests", "golden", "coefficients.json")) as f:
+        c = json.load(f)["coeffs3d"][spec["gold"]]
+    r = spec["r"]
+    cube = np.zeros((2 * r + 1,) * 3)
+    for k, v in c.items():
+        cube[int(k[0]), int(k[1]), int(k[2])] = v
+    return cube / cube.sum()
+
+
 def coefficients(spec):
     """Coefficients uniform[0,1) normalised to sum 1 (seeded)."""
     if "coeffs" in spec:
         return spec["coeffs"]
+    if spec["kind"] == "3d":
+        return cube3d(spec)
     g = np.random.Generator(np.random.PCG64(1234 + spec["r"]))
     c = g.random(taps(spec))
     return list(c / c.sum())
@@ -184,6 +208,21 @@ def cpu_reference_rate(spec, budget_s: float, seed: int = 7):
     dt = np_dtype(spec["dtype"]) or np.float32
     n = spec["n"]
     g = np.random.Generator(np.random.PCG64(seed))
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    if spec["kind"] == "3d":
+        # the reference gold for this stencil (v2::j3d7pt_gold / j3d13pt_gold /
+        # poisson_gold), iterated with copy-back like its IT-step check
+        cur = g.random((n, n, n), dtype=np.float32).astype(dt)
+        t0 = time.perf_counter()
+        done = 0
+        while True:
+            cur = oracle.ref_gold3d(spec["gold"], cur)
+            done += 1
+            el = time.perf_counter() - t0
+            if el >= budget_s or done >= spec["steps"]:
+                break
+        sample = f"{done} of {spec['steps']} step(s) on the full {n}^3 grid"
+        return n ** 3 * done / el / 1e9, sample, cores
     c = coefficients(spec)
     if spec["kind"] == "star":
         r = spec["r"]
@@ -224,7 +263,6 @@ def cpu_reference_rate(spec, budget_s: float, seed: int = 7):
         el = time.perf_counter() - t0
         cells = rows * n * steps
         sample = f"{rows}-row slab of the {n}x{n} grid x {steps} step(s)"
-    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     return cells / el / 1e9, sample, cores
 
 
@@ -243,14 +281,15 @@ def run_reference(args, spec, name):
         if i >= args.warmup:
             rates.append(rate)
     value = statistics.median(rates) if rates else None
-    cells = spec["n"] ** 2 * spec["steps"]
+    nd = 3 if spec["kind"] == "3d" else 2
+    cells = spec["n"] ** nd * spec["steps"]
     line = {
         "impl": "reference", "metric": "GCells/s", "value": value, "unit": "GCells/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": (cells / (value * 1e9) * 1e3) if value else None,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": spec["dtype"], "data": "synthetic (seeded uniform[-1,1))",
-        "config": dict(workload=name, grid=f"{spec['n']}x{spec['n']}", kind=spec["kind"],
+        "config": dict(workload=name, grid="x".join([str(spec["n"])] * nd), kind=spec["kind"],
                        radius=spec["r"], steps_per_call=spec["steps"],
                        boundary=spec["boundary"]),
         "cpu_baseline": {"value": value, "unit": "GCells/s", "cores": cores,
@@ -280,15 +319,17 @@ def run_ssam(args, spec, name):
                                 device_id=dev)
 
     n = spec["n"]
+    kind = spec["kind"]
     tdt = {"f32": torch.float32, "f64": torch.float64, "bf16": torch.bfloat16}[spec["dtype"]]
     gen = torch.Generator(device=dev)
     gen.manual_seed(1000 + rank)
-    srcs = [(torch.rand(n, n, device=dev, dtype=torch.float32, generator=gen) * 2 - 1).to(tdt)
-            for _ in range(2)]
+    dims = (n, n, n) if kind == "3d" else (n, n)
+    lo = 0.0 if kind == "3d" else -1.0  # 3D: uniform[0,1); 2D: uniform[-1,1)
+    srcs = [(torch.rand(*dims, device=dev, dtype=torch.float32, generator=gen) * (1 - lo)
+             + lo).to(tdt) for _ in range(2)]
     dst = torch.empty_like(srcs[0])
     c = coefficients(spec)
     r = spec["r"]
-    kind = spec["kind"]
     shape = S.STAR if kind == "star" else S.BOX
     stream = torch.cuda.current_stream(dev)
 
@@ -297,6 +338,12 @@ def run_ssam(args, spec, name):
 
         def step(i):
             S.conv2d(srcs[i % 2], w, boundary=spec["boundary"], dst=dst, stream=stream)
+    elif kind == "3d":
+        shape = S.POISSON19 if spec["gold"] == "poisson" else S.STAR3D
+
+        def step(i):
+            S.stencil3d(srcs[i % 2], c, r, shape, steps=spec["steps"],
+                        boundary=spec["boundary"], dst=dst, stream=stream)
     else:
         def step(i):
             S.stencil2d(srcs[i % 2], c, r, shape, steps=spec["steps"],
@@ -337,32 +384,33 @@ def run_ssam(args, spec, name):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = t.item()
 
-    cells = n * n * spec["steps"]
+    cells = n ** len(dims) * spec["steps"]
     value = cells * args.steps * world / (total_ms / 1e3) / 1e9
     es = elem_size(spec["dtype"])
     # launches per call: one per chained temporal block (counted by the library)
     launches_per_step = max(1, launches // args.steps)
     peak, peak_kind = load_peaks()
     # algorithmic bytes of one call: read + write each cell once per launch
-    alg_bytes = 2 * n * n * es * launches_per_step
+    alg_bytes = 2 * n ** len(dims) * es * launches_per_step
     achieved = alg_bytes / (avg_launch_ms / 1e3) / 1e9
     traffic = load_traffic(name)
 
     # end to end: host buffers through ssam_stencil2d_host, copies timed
     e2e = None
     if kind != "conv":
+        host_call = S.stencil3d_host if kind == "3d" else S.stencil2d_host
         k_e2e = max(3, min(args.steps, 20))
         hs = srcs[0].cpu().pin_memory()
         hd = torch.empty_like(hs).pin_memory()
         for _ in range(2):
-            S.stencil2d_host(hs, hd, c, r, shape, spec["steps"], spec["boundary"], dev, stream)
+            host_call(hs, hd, c, r, shape, spec["steps"], spec["boundary"], dev, stream)
         torch.cuda.synchronize()
         barrier()
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record(stream)
         for _ in range(k_e2e):
-            S.stencil2d_host(hs, hd, c, r, shape, spec["steps"], spec["boundary"], dev, stream)
+            host_call(hs, hd, c, r, shape, spec["steps"], spec["boundary"], dev, stream)
         b.record(stream)
         torch.cuda.synchronize()
         e_ms = a.elapsed_time(b)
@@ -371,7 +419,8 @@ def run_ssam(args, spec, name):
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             e_ms = t.item()
         e2e = {"value": cells * k_e2e * world / (e_ms / 1e3) / 1e9, "unit": "GCells/s",
-               "h2d_bytes_per_step": n * n * es, "d2h_bytes_per_step": n * n * es,
+               "h2d_bytes_per_step": n ** len(dims) * es,
+               "d2h_bytes_per_step": n ** len(dims) * es,
                "steps": k_e2e}
 
     cpu = None
@@ -391,11 +440,12 @@ def run_ssam(args, spec, name):
             "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": spec["dtype"],
             "data": "synthetic (seeded uniform[-1,1), coefficients uniform[0,1) normalised)",
-            "config": {"workload": name, "grid": f"{n}x{n}", "kind": kind, "radius": r,
+            "config": {"workload": name, "grid": "x".join([str(n)] * len(dims)), "kind": kind,
+                       "radius": r,
                        "taps": taps(spec), "steps_per_call": spec["steps"],
                        "boundary": spec["boundary"],
                        "l2": "inputs larger than L2: two alternating "
-                             f"{n * n * es / 2**20:.0f} MiB inputs + output vs 126 MB L2",
+                             f"{n ** len(dims) * es / 2**20:.0f} MiB inputs + output vs 126 MB L2",
                        "parallelism": f"dp{world} (independent grid per GPU)"},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,

@@ -91,6 +91,17 @@ typedef enum ssam_shape2d {
   SSAM_BOX = 1
 } ssam_shape2d;
 
+/* Tap pattern of a 3D stencil of radius r (coefficients are always passed as
+ * the dense (2r+1)^3 cube, see ssam_stencil3d). */
+typedef enum ssam_shape3d {
+  /* taps on the three axes: 7-pt (r=1, tmp3d7pt-v2.cu) and 13-pt (r=2,
+   * tmp3d13pt.cu) */
+  SSAM_STAR3D = 0,
+  /* r=1, every tap with at most two non-zero offsets: the reference's 19-point
+   * "poisson" operator (tmpPoisson.cu:369-386) */
+  SSAM_POISSON19 = 2
+} ssam_shape3d;
+
 /* ---------------------------------------------------------------- library */
 
 /* Message for the calling thread's most recent non-OK status ("" if none). */
@@ -166,6 +177,44 @@ SSAM_API int ssam_stencil2d_host(const void* h_src, void* h_dst, int64_t width,
 SSAM_API int ssam_conv2d(const void* src, void* dst, int64_t width, int64_t pitch,
                 int64_t height, int dtype, const double* weight, int fw, int fh,
                 int boundary, void* stream);
+
+/* ------------------------------------------------------------ 3D stencils */
+
+/*
+ * `steps` time steps of a 3D stencil on a dense nx*ny*nz grid
+ * (index nx*ny*z + nx*y + x).
+ *
+ * Replaces v2::kernel3d_3d7pt (ssai-3dstencil/tmp3d7pt-v2.cu:62-208),
+ * kernel3d_3d13pt (tmp3d13pt.cu:74-230), kernel3d_poisson
+ * (tmpPoisson.cu:86-298), their host_code drivers and the entry points
+ * stencil_3d7pt_v2 / stencil_3d13pt / stencil_poisson (ssai-3dstencil/
+ * main.cpp:5-21).
+ *
+ * coeffs: the dense (2r+1)^3 cube, coeffs[((dz+r)*(2r+1) + dy+r)*(2r+1) + dx+r]
+ * weights in(z+dz, y+dy, x+dx) -- the reference's `_F<z><y><x>` defines with
+ * digits = offset + r (tmp3d7pt-v2.cu:9-15).  Entries outside the shape's
+ * pattern are ignored.  Supported: SSAM_STAR3D r = 1, 2 and SSAM_POISSON19.
+ * boundary: ZERO or COPY (the reference golds' interior with the ring kept).
+ * steps > 1 chain through a stream-ordered scratch grid; unless the stream is
+ * already being captured, the whole chain is captured once into a CUDA graph
+ * (cached per pointers/sizes/coefficients) and replayed on later calls.
+ */
+SSAM_API int ssam_stencil3d(const void* src, void* dst, int64_t nx, int64_t ny, int64_t nz,
+                            int dtype, int shape, int radius, const double* coeffs,
+                            int steps, int boundary, void* stream);
+
+/* ssam_stencil3d on HOST buffers (copy in, steps, copy out, on `stream`). */
+SSAM_API int ssam_stencil3d_host(const void* h_src, void* h_dst, int64_t nx, int64_t ny,
+                                 int64_t nz, int dtype, int shape, int radius,
+                                 const double* coeffs, int steps, int boundary,
+                                 void* stream);
+
+/*
+ * Synchronises `stream` and reports whether a bounded device-side wait of
+ * any kernel on the current device gave up since the last call
+ * (SSAM_ERR_TIMEOUT, with the code in the message); clears the flag.
+ */
+SSAM_API int ssam_device_status(void* stream);
 
 #ifdef __cplusplus
 }

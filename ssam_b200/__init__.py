@@ -51,6 +51,14 @@ def _declare(lib):
                                    _int, _int, _vp]
     lib.ssam_stencil2d_host.restype = _int
     lib.ssam_stencil2d_host.argtypes = lib.ssam_stencil2d.argtypes
+    lib.ssam_stencil3d.restype = _int
+    lib.ssam_stencil3d.argtypes = [_vp, _vp, _i64, _i64, _i64, _int, _int, _int, _dp, _int,
+                                   _int, _vp]
+    lib.ssam_stencil3d_host.restype = _int
+    lib.ssam_stencil3d_host.argtypes = lib.ssam_stencil3d.argtypes
+    lib.ssam_device_status.restype = _int
+    lib.ssam_device_status.argtypes = [_vp]
+    lib.ssam_trim_scratch.restype = _int
     lib.ssam_conv2d.restype = _int
     lib.ssam_conv2d.argtypes = [_vp, _vp, _i64, _i64, _i64, _int, _dp, _int, _int,
                                 _int, _vp]
@@ -156,6 +164,63 @@ def conv2d(src, weight, boundary: str = "zero", dst=None, stream=None):
                              _dtype_code(src), c, fw, fh, BOUNDARY[boundary],
                              _stream_ptr(src, stream)))
     return dst
+
+
+STAR3D, POISSON19 = 0, 2
+
+
+def _grid3d(src, dst):
+    import torch
+    if not src.is_cuda:
+        raise ValueError("src must be a CUDA tensor")
+    if src.dim() != 3 or not src.is_contiguous():
+        raise ValueError("3D grids must be contiguous (nz, ny, nx) tensors")
+    if dst is None:
+        dst = torch.empty_like(src)
+    if dst.shape != src.shape or dst.dtype != src.dtype or not dst.is_contiguous():
+        raise ValueError("dst must match src")
+    return dst
+
+
+def stencil3d(src, coeffs, radius: int = 1, shape: int = STAR3D, steps: int = 1,
+              boundary: str = "zero", dst=None, stream=None):
+    """``steps`` steps of a 3D stencil (``ssam_stencil3d``); ``coeffs`` is the
+    dense (2r+1)^3 cube indexed [dz+r][dy+r][dx+r] (any array-like)."""
+    dst = _grid3d(src, dst)
+    nz, ny, nx = src.shape
+    flat = coeffs.ravel().tolist() if hasattr(coeffs, "ravel") else list(coeffs)
+    c = _doubles(flat)
+    _check(lib().ssam_stencil3d(src.data_ptr(), dst.data_ptr(), nx, ny, nz, _dtype_code(src),
+                                shape, radius, c, steps, BOUNDARY[boundary],
+                                _stream_ptr(src, stream)))
+    return dst
+
+
+def stencil3d_host(src, dst, coeffs, radius: int = 1, shape: int = STAR3D, steps: int = 1,
+                   boundary: str = "zero", device=None, stream=None):
+    """``ssam_stencil3d_host`` on (pinned) CPU tensors; synchronise before
+    reading ``dst``."""
+    import torch
+    if src.is_cuda or dst.is_cuda or src.shape != dst.shape or src.dim() != 3:
+        raise ValueError("stencil3d_host takes matching 3D host tensors")
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    if stream is None:
+        stream = torch.cuda.current_stream(dev)
+    nz, ny, nx = src.shape
+    flat = coeffs.ravel().tolist() if hasattr(coeffs, "ravel") else list(coeffs)
+    with torch.cuda.device(dev):
+        _check(lib().ssam_stencil3d_host(src.data_ptr(), dst.data_ptr(), nx, ny, nz,
+                                         _dtype_code(src), shape, radius, _doubles(flat),
+                                         steps, BOUNDARY[boundary],
+                                         ctypes.c_void_p(stream.cuda_stream)))
+    return dst
+
+
+def device_status(stream=None) -> None:
+    """Raise SsamError(SSAM_ERR_TIMEOUT) if a bounded device wait gave up."""
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    _check(lib().ssam_device_status(ctypes.c_void_p(s.cuda_stream)))
 
 
 def star_coeffs_from_matrix(m) -> list[float]:

@@ -419,6 +419,82 @@ int ssam_stencil2d_host(const void* h_src, void* h_dst, int64_t width, int64_t h
                      (cudaStream_t)stream);
 }
 
+static int check_3d(const void* src, const void* dst, int64_t nx, int64_t ny, int64_t nz,
+                    int dtype, int shape, int radius, const double* coeffs, int steps,
+                    int boundary) {
+  if (!src || !dst) return fail(SSAM_ERR_INVALID, "src and dst must not be NULL");
+  if (nx < 1 || ny < 1 || nz < 1) return fail(SSAM_ERR_INVALID, "nx, ny, nz must be >= 1");
+  if (nx > (int64_t(1) << 31) || ny > (int64_t(1) << 31) || nz > (int64_t(1) << 31))
+    return fail(SSAM_ERR_INVALID, "grid side above 2^31");
+  if (!valid_dtype(dtype)) return fail(SSAM_ERR_INVALID, "unknown dtype");
+  if (shape != SSAM_STAR3D && shape != SSAM_POISSON19)
+    return fail(SSAM_ERR_INVALID, "shape must be SSAM_STAR3D or SSAM_POISSON19");
+  if (radius < 1 || radius > 4 || (shape == SSAM_POISSON19 && radius != 1))
+    return fail(SSAM_ERR_INVALID, "radius must be 1..4 (POISSON19: 1)");
+  if (!coeffs) return fail(SSAM_ERR_INVALID, "coeffs must not be NULL");
+  if (steps < 1) return fail(SSAM_ERR_INVALID, "steps must be >= 1");
+  if (boundary != SSAM_BOUNDARY_ZERO && boundary != SSAM_BOUNDARY_COPY)
+    return fail(boundary == SSAM_BOUNDARY_CLAMP ? SSAM_ERR_UNSUPPORTED : SSAM_ERR_INVALID,
+                "3D boundary must be ZERO or COPY");
+  const uintptr_t len = (uintptr_t)(nx * ny * nz) * dtype_size(dtype);
+  if ((uintptr_t)src < (uintptr_t)dst + len && (uintptr_t)dst < (uintptr_t)src + len)
+    return fail(SSAM_ERR_INVALID, "src and dst overlap (updates are out of place)");
+  return SSAM_OK;
+}
+
+int ssam_stencil3d(const void* src, void* dst, int64_t nx, int64_t ny, int64_t nz,
+                   int dtype, int shape, int radius, const double* coeffs, int steps,
+                   int boundary, void* stream) {
+  int st = check_3d(src, dst, nx, ny, nz, dtype, shape, radius, coeffs, steps, boundary);
+  if (st != SSAM_OK) return st;
+  return run_3d(src, dst, nx, ny, nz, dtype, shape == SSAM_POISSON19 ? 1 : 0, radius,
+                coeffs, steps, boundary, 1, (cudaStream_t)stream);
+}
+
+int ssam_stencil3d_host(const void* h_src, void* h_dst, int64_t nx, int64_t ny, int64_t nz,
+                        int dtype, int shape, int radius, const double* coeffs, int steps,
+                        int boundary, void* stream) {
+  int st = check_3d(h_src, h_dst, nx, ny, nz, dtype, shape, radius, coeffs, steps, boundary);
+  if (st != SSAM_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t bytes = (size_t)(nx * ny * nz) * dtype_size(dtype);
+  void* d_src = nullptr;
+  void* d_dst = nullptr;
+  st = scratch_alloc(&d_src, bytes, s);
+  if (st == SSAM_OK) st = scratch_alloc(&d_dst, bytes, s);
+  if (st == SSAM_OK) {
+    cudaError_t e = cudaMemcpyAsync(d_src, h_src, bytes, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) st = fail_cuda(e, "host-to-device copy");
+  }
+  // plain launches: the device buffers change from call to call
+  if (st == SSAM_OK)
+    st = run_3d(d_src, d_dst, nx, ny, nz, dtype, shape == SSAM_POISSON19 ? 1 : 0, radius,
+                coeffs, steps, boundary, 0, s);
+  if (st == SSAM_OK) {
+    cudaError_t e = cudaMemcpyAsync(h_dst, d_dst, bytes, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) st = fail_cuda(e, "device-to-host copy");
+  }
+  scratch_free(d_src, s);
+  scratch_free(d_dst, s);
+  return st;
+}
+
+int ssam_device_status(void* stream) {
+  SSAM_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  int* word = nullptr;
+  int st = device_error_word(&word);
+  if (st != SSAM_OK) return st;
+  int v = 0;
+  SSAM_CUDA_TRY(cudaMemcpy(&v, word, sizeof(int), cudaMemcpyDeviceToHost));
+  if (v != 0) {
+    const int zero = 0;
+    SSAM_CUDA_TRY(cudaMemcpy(word, &zero, sizeof(int), cudaMemcpyHostToDevice));
+    return fail(SSAM_ERR_TIMEOUT, "a bounded device wait gave up (code " + std::to_string(v) +
+                                      ": 1 producer/empty, 2 drain, 3 consumer/full)");
+  }
+  return SSAM_OK;
+}
+
 int ssam_conv2d(const void* src, void* dst, int64_t width, int64_t pitch,
                 int64_t height, int dtype, const double* weight, int fw, int fh,
                 int boundary, void* stream) {

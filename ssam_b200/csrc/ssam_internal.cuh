@@ -24,6 +24,12 @@ int fail_cuda(cudaError_t e, const char* what);
 // Process-wide count of kernel launches (ssam_kernel_launches).
 void count_launch();
 
+// 3D path (stencil3d.cu).  shape: 0 = star, 1 = 19-point.
+int run_3d(const void* src, void* dst, int64_t nx, int64_t ny, int64_t nz, int dtype,
+           int shape, int r, const double* coef, int steps, int boundary, int use_graph,
+           cudaStream_t stream);
+int device_error_word(int** out);
+
 // Stream-ordered device scratch from the library's per-device pool.
 int scratch_alloc(void** p, size_t bytes, cudaStream_t s);
 void scratch_free(void* p, cudaStream_t s);
@@ -109,6 +115,13 @@ __device__ __forceinline__ void store_vec(TS* __restrict__ p, const TA (&r)[V]) 
     reinterpret_cast<uint4*>(p)[c] = u;
   }
 }
+
+// Coefficients passed by value as a kernel parameter (constant bank), indexed
+// with compile-time offsets by the unrolled kernels.
+template <typename TA, int N>
+struct CoefBlock {
+  TA c[N];
+};
 
 // ---------------------------------------------------------- kernel registry --
 

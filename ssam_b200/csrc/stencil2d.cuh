@@ -36,11 +36,6 @@
 
 namespace ssam {
 
-template <typename TA, int N>
-struct CoefBlock {
-  TA c[N];
-};
-
 template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int P, int T>
 struct Stencil2DCfg {
   using TA = typename Traits<TS>::TA;
@@ -71,6 +66,30 @@ __device__ __forceinline__ TA fix_cell(TA v, int64_t y, int64_t x, int64_t W,
       ((x < rl) | (x >= W - rr) | (y < rt) | (y >= H - rb)))
     return to_acc(src[y * pitch + x]);
   return v;
+}
+
+// Row load/store for a lane whose V columns are not all inside [0, W) or not
+// 16-byte aligned: per element, with the boundary rule for columns outside.
+template <typename TS, int V, typename TA>
+__device__ __forceinline__ void load_row_edge(TA (&d)[V], const TS* __restrict__ row,
+                                              int64_t x0, int64_t W, int bnd) {
+#pragma unroll
+  for (int j = 0; j < V; ++j) {
+    int64_t x = x0 + j;
+    if ((x < 0 || x >= W) && bnd == SSAM_BOUNDARY_ZERO) {
+      d[j] = TA(0);
+    } else {
+      x = x < 0 ? 0 : (x >= W ? W - 1 : x);
+      d[j] = to_acc(row[x]);
+    }
+  }
+}
+template <typename TS, int V, typename TA>
+__device__ __forceinline__ void store_row_edge(TS* __restrict__ row, int64_t x0, int64_t W,
+                                               const TA (&d)[V]) {
+#pragma unroll
+  for (int j = 0; j < V; ++j)
+    if (x0 + j < W) row[x0 + j] = from_acc<TS>(d[j]);
 }
 
 template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int P, int T>
@@ -111,30 +130,49 @@ stencil2d_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int64_t W,
     // ---- register cache: ROWS rows x V columns, 16-byte loads ----------
     TA d[ROWS][V];
     const bool row_vec = vec_ok && x0 >= 0 && x0 + V <= W;
+    // Three separate load loops: a branch inside one unrolled loop makes the
+    // compiler keep every path's loads live at once (2-4x the registers).
+    if (row_vec && y0 >= 0 && y0 + ROWS <= H) {
+      // interior: 16-byte loads, one pointer increment per row
+      const TS* p = src + y0 * pitch + x0;
 #pragma unroll
-    for (int k = 0; k < ROWS; ++k) {
-      int64_t y = y0 + k;
-      const bool yin = y >= 0 && y < H;
-      if (!yin && bnd == SSAM_BOUNDARY_ZERO) {
-#pragma unroll
-        for (int j = 0; j < V; ++j) d[k][j] = TA(0);
-        continue;
+      for (int k = 0; k < ROWS; ++k) {
+        load_vec<TS, V>(d[k], p);
+        p += pitch;
       }
-      y = y < 0 ? 0 : (y >= H ? H - 1 : y);
-      const TS* row = src + y * pitch;
-      if (row_vec) {
-        load_vec<TS, V>(d[k], row + x0);
-      } else {
+    } else if (row_vec) {
+      // rows beyond the top/bottom edge: zero or clamped row
 #pragma unroll
-        for (int j = 0; j < V; ++j) {
-          int64_t x = x0 + j;
-          if ((x < 0 || x >= W) && bnd == SSAM_BOUNDARY_ZERO) {
-            d[k][j] = TA(0);
-          } else {
-            x = x < 0 ? 0 : (x >= W ? W - 1 : x);
-            d[k][j] = to_acc(row[x]);
-          }
+      for (int k = 0; k < ROWS; ++k) {
+        int64_t y = y0 + k;
+        if ((y < 0 || y >= H) && bnd == SSAM_BOUNDARY_ZERO) {
+#pragma unroll
+          for (int j = 0; j < V; ++j) d[k][j] = TA(0);
+        } else {
+          y = y < 0 ? 0 : (y >= H ? H - 1 : y);
+          load_vec<TS, V>(d[k], src + y * pitch + x0);
         }
+      }
+    } else {
+      // columns beyond the left/right edge or unaligned grid: per element
+#pragma unroll 1
+      for (int k = 0; k < ROWS; ++k) {
+        int64_t y = y0 + k;
+        TA v[V];
+        if ((y < 0 || y >= H) && bnd == SSAM_BOUNDARY_ZERO) {
+#pragma unroll
+          for (int j = 0; j < V; ++j) v[j] = TA(0);
+        } else {
+          y = y < 0 ? 0 : (y >= H ? H - 1 : y);
+          load_row_edge<TS, V>(v, src + y * pitch, x0, W, bnd);
+        }
+        // rotate the window so that the row can land in a static slot
+#pragma unroll
+        for (int r = 0; r < ROWS - 1; ++r)
+#pragma unroll
+          for (int j = 0; j < V; ++j) d[r][j] = d[r + 1][j];
+#pragma unroll
+        for (int j = 0; j < V; ++j) d[ROWS - 1][j] = v[j];
       }
     }
 
@@ -251,18 +289,14 @@ stencil2d_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int64_t W,
 
     // ---- store P rows from the strip's interior lanes ------------------
     if (lane_stores) {
+      TS* p = dst + y_out0 * pitch;
 #pragma unroll
       for (int i = 0; i < P; ++i) {
-        const int64_t y = y_out0 + i;
-        if (y >= y_end) break;
-        TS* row = dst + y * pitch;
-        if (row_vec) {
-          store_vec<TS, V>(row + x0, d[i]);
-        } else {
-#pragma unroll
-          for (int j = 0; j < V; ++j)
-            if (x0 + j < W) row[x0 + j] = from_acc<TS>(d[i][j]);
+        if (y_out0 + i < y_end) {
+          if (row_vec) store_vec<TS, V>(p + x0, d[i]);
+          else store_row_edge<TS, V>(p, x0, W, d[i]);
         }
+        p += pitch;
       }
     }
   }

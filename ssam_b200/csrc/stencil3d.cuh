@@ -1,0 +1,434 @@
+// 3D stencils for sm_100a: persistent z-marching CTAs fed by TMA.
+//
+// Method (the reference's 3D scheme, ssai-3dstencil/tmp3d7pt-v2.cu:62-208:
+// "y-strip in registers, x by shuffles, z through shared memory"), laid out
+// for Blackwell:
+//   * a CTA owns column tiles of 128 x TY cells and walks them along z.  A
+//     producer warp stages each z-plane of the tile -- 128 + 2*HX columns by
+//     TY + 2*RY rows, halos included -- into a ring of S shared-memory slots
+//     with one cp.async.bulk.tensor (TMA, no multicast) per plane, signalled
+//     through mbarriers (full: bytes landed; empty: consumers are done);
+//   * NW consumer warps each own a 128 x PY strip.  A thread owns V = 4
+//     consecutive columns; for every plane of the stencil it reads its rows
+//     (plus the y reach) from the slot into registers, forms its own
+//     contributions and the partial sums destined for the neighbouring
+//     lanes' columns, and the partial sums move one lane downstream with
+//     __shfl_up/down_sync (lanes 0 and 31 take theirs from the slot's halo
+//     columns instead);
+//   * z-neighbours are read from the slots of the adjacent planes (shared
+//     memory between warps, as in the reference);
+//   * work is split evenly over a persistent grid as contiguous runs of
+//     (column tile, plane) pairs, so the grid is sized to the SM count and no
+//     tile restarts more than once;
+//   * every mbarrier wait is bounded (%globaltimer): on expiry the kernel
+//     records an error code, the producer drains its own copies in flight
+//     (again bounded), and the CTA returns.
+//
+// Shapes: STAR (7-pt r=1, 13-pt r=2, ...: taps on the three axes) and
+// POISSON19 (all taps with |d|_inf <= 1 and |d|_1 <= 2: the reference's
+// 19-point operator, tmpPoisson.cu:369-386).
+#pragma once
+
+#include <cuda.h>
+
+#include "ssam_internal.cuh"
+
+namespace ssam {
+
+enum { SH3_STAR = 0, SH3_POISSON19 = 1 };
+
+__host__ __device__ constexpr int iabs_(int v) { return v < 0 ? -v : v; }
+
+template <int SH, int R>
+__host__ __device__ constexpr bool tap3(int dz, int dy, int dx) {
+  return SH == SH3_STAR
+             ? ((dy == 0 && dx == 0) || (dz == 0 && dx == 0) || (dz == 0 && dy == 0))
+             : (iabs_(dz) <= 1 && iabs_(dy) <= 1 && iabs_(dx) <= 1 &&
+                iabs_(dz) + iabs_(dy) + iabs_(dx) <= 2);
+}
+
+// y reach needed in plane dz; x reach needed in row (dz, dy).
+template <int SH, int R>
+__host__ __device__ constexpr int ry3(int dz) {
+  int m = -1;
+  for (int dy = -R; dy <= R; ++dy)
+    for (int dx = -R; dx <= R; ++dx)
+      if (tap3<SH, R>(dz, dy, dx) && iabs_(dy) > m) m = iabs_(dy);
+  return m;  // -1: plane unused
+}
+template <int SH, int R>
+__host__ __device__ constexpr int rx3(int dz, int dy) {
+  int m = -1;
+  for (int dx = -R; dx <= R; ++dx)
+    if (tap3<SH, R>(dz, dy, dx) && iabs_(dx) > m) m = iabs_(dx);
+  return m;
+}
+
+template <typename TS, int SH, int R, int PY, int NW, int S>
+struct Stencil3DCfg {
+  using TA = typename Traits<TS>::TA;
+  static constexpr int V = 4;                       // columns per thread
+  static constexpr int TX = 128;                    // tile columns
+  static constexpr int HX = 16 / (int)sizeof(TS);   // halo columns (16 bytes)
+  static constexpr int TY = NW * PY;                // tile rows
+  static constexpr int RYM = ry3<SH, R>(0) > 0 ? ry3<SH, R>(0) : 1;  // max y reach
+  static constexpr int XW = TX + 2 * HX;            // slot row length
+  static constexpr int YW = TY + 2 * RYM;           // slot rows
+  static constexpr int SLOT_BYTES = ((XW * YW * (int)sizeof(TS)) + 127) / 128 * 128;
+  static constexpr int SMEM = S * SLOT_BYTES + 2 * S * 8 + 128;
+  static constexpr int NC = (2 * R + 1) * (2 * R + 1) * (2 * R + 1);
+  static constexpr int THREADS = 32 * (NW + 1);
+  static_assert(R <= HX && R <= V, "x reach must fit in the halo and one lane hop");
+  static_assert(S >= 2 * R + 2, "ring must hold the stencil window plus one plane");
+};
+
+struct Work3D {
+  int64_t nx, ny, nz;
+  int ntx, nty;          // column tiles
+  int64_t total;         // ntx*nty*nz (tile, plane) pairs
+  int64_t per_cta;       // contiguous pairs per CTA
+  int boundary;
+  int use_tma;
+  unsigned long long wait_ns;
+  int* err;              // device error word (0 = ok)
+};
+
+// ------------------------------------------------------------ PTX helpers --
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ uint64_t gtimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mbar_init(uint64_t* b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)),
+               "r"(bytes)
+               : "memory");
+}
+// Waits for the phase with parity `par` to complete; false after `ns`.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned par, unsigned long long ns) {
+  const uint32_t a = smem_u32(b);
+  uint32_t ok = 0;
+  asm volatile(
+      "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; "
+      "selp.u32 %0, 1, 0, p; }"
+      : "=r"(ok)
+      : "r"(a), "r"(par)
+      : "memory");
+  if (ok) return true;
+  const uint64_t t0 = gtimer();
+  while (true) {
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; "
+        "selp.u32 %0, 1, 0, p; }"
+        : "=r"(ok)
+        : "r"(a), "r"(par)
+        : "memory");
+    if (ok) return true;
+    if (gtimer() - t0 > ns) return false;
+  }
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y,
+                                            int z, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// V elements of a staged plane row (16-byte aligned for 4- and 8-byte types,
+// 8-byte aligned for 2-byte types).
+template <typename TS, int V, typename TA>
+__device__ __forceinline__ void load_slot_row(TA (&d)[V], const TS* p) {
+  constexpr int B = V * (int)sizeof(TS);
+  if constexpr (B % 16 == 0) {
+#pragma unroll
+    for (int c = 0; c < B / 16; ++c) {
+      const uint4 u = reinterpret_cast<const uint4*>(p)[c];
+      const TS* e = reinterpret_cast<const TS*>(&u);
+#pragma unroll
+      for (int k = 0; k < 16 / (int)sizeof(TS); ++k) d[c * (16 / sizeof(TS)) + k] = to_acc(e[k]);
+    }
+  } else if constexpr (B == 8) {
+    const uint2 u = *reinterpret_cast<const uint2*>(p);
+    const TS* e = reinterpret_cast<const TS*>(&u);
+#pragma unroll
+    for (int k = 0; k < V; ++k) d[k] = to_acc(e[k]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < V; ++k) d[k] = to_acc(p[k]);
+  }
+}
+
+template <typename TS, int V, typename TA>
+__device__ __forceinline__ void store_row(TS* p, const TA (&o)[V]) {
+  constexpr int B = V * (int)sizeof(TS);
+  if constexpr (B % 16 == 0) {
+    store_vec<TS, V>(p, o);
+  } else if constexpr (B == 8) {
+    uint2 u;
+    TS* e = reinterpret_cast<TS*>(&u);
+#pragma unroll
+    for (int k = 0; k < V; ++k) e[k] = from_acc<TS>(o[k]);
+    *reinterpret_cast<uint2*>(p) = u;
+  } else {
+#pragma unroll
+    for (int k = 0; k < V; ++k) p[k] = from_acc<TS>(o[k]);
+  }
+}
+
+// Segment = run of consecutive planes [za, zb) of one column tile.
+struct Seg3D {
+  int64_t tile, za, zb;
+};
+__device__ __forceinline__ bool next_seg(int64_t& pos, int64_t end, int64_t nz, Seg3D& s) {
+  if (pos >= end) return false;
+  s.tile = pos / nz;
+  s.za = pos % nz;
+  const int64_t tile_end = (s.tile + 1) * nz;
+  const int64_t stop = end < tile_end ? end : tile_end;
+  s.zb = s.za + (stop - pos);
+  pos = stop;
+  return true;
+}
+
+template <typename TS, int SH, int R, int PY, int NW, int S>
+__global__ void __launch_bounds__(32 * (NW + 1), 1)
+stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__ src,
+                 TS* __restrict__ dst, Work3D w,
+                 CoefBlock<typename Traits<TS>::TA,
+                           Stencil3DCfg<TS, SH, R, PY, NW, S>::NC> cf) {
+  using C = Stencil3DCfg<TS, SH, R, PY, NW, S>;
+  using TA = typename C::TA;
+  constexpr int V = C::V, XW = C::XW, HX = C::HX, RYM = C::RYM, TY = C::TY;
+  constexpr int F = 2 * R + 1;
+  constexpr unsigned FULL = 0xffffffffu;
+
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char* base =
+      (unsigned char*)(((uintptr_t)smem_raw + 127) & ~(uintptr_t)127);
+  TS* slots = (TS*)base;
+  uint64_t* full = (uint64_t*)(base + S * C::SLOT_BYTES);
+  uint64_t* empty = full + S;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], w.use_tma ? 1u : 32u);
+      mbar_init(&empty[s], (unsigned)NW);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+
+  const int64_t begin = (int64_t)blockIdx.x * w.per_cta;
+  const int64_t end = begin + w.per_cta < w.total ? begin + w.per_cta : w.total;
+  const int64_t nx = w.nx, ny = w.ny, nz = w.nz, nxy = nx * ny;
+
+  if (warp == NW) {
+    // ------------------------------------------------------ producer warp
+    uint32_t n = 0;  // planes issued so far (ring position)
+    bool ok = true;
+    int64_t pos = begin;
+    Seg3D sg;
+    while (ok && next_seg(pos, end, nz, sg)) {
+      const int tx = (int)(sg.tile % w.ntx), ty = (int)(sg.tile / w.ntx);
+      const int gx = tx * C::TX - HX, gy = ty * TY - RYM;
+      for (int64_t p = sg.za - R; p < sg.zb + R; ++p, ++n) {
+        const int s = n % S;
+        const unsigned use = n / S;
+        if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1, w.wait_ns)) {
+          if (lane == 0) atomicCAS(w.err, 0, 1);
+          ok = false;
+          break;
+        }
+        TS* slot = slots + (size_t)s * (C::SLOT_BYTES / sizeof(TS));
+        if (w.use_tma) {
+          if (lane == 0) {
+            mbar_expect_tx(&full[s], (unsigned)(XW * C::YW * sizeof(TS)));
+            tma_load_3d(slot, &map, gx, gy, (int)p, &full[s]);
+          }
+        } else {
+          // plain loads for grids whose rows are not 16-byte multiples
+          for (int i = lane; i < XW * C::YW; i += 32) {
+            const int r = i / XW, c = i % XW;
+            const int64_t x = gx + c, y = gy + r;
+            TS v = from_acc<TS>(TA(0));
+            if (x >= 0 && x < nx && y >= 0 && y < ny && p >= 0 && p < nz)
+              v = src[p * nxy + y * nx + x];
+            slot[r * XW + c] = v;
+          }
+          mbar_arrive(&full[s]);
+        }
+        __syncwarp();
+      }
+    }
+    // drain: the last use of every slot must have landed before exit
+    if (w.use_tma && lane == 0) {
+      const uint32_t first = n > (uint32_t)S ? n - S : 0;
+      for (uint32_t k = first; k < n; ++k)
+        if (!mbar_wait(&full[k % S], (k / S) & 1, w.wait_ns)) atomicCAS(w.err, 0, 2);
+    }
+    return;
+  }
+
+  // --------------------------------------------------------- consumer warps
+  uint32_t n = 0;  // ring position of the segment's first plane
+  int64_t pos = begin;
+  Seg3D sg;
+  while (next_seg(pos, end, nz, sg)) {
+    const int tx = (int)(sg.tile % w.ntx), ty = (int)(sg.tile / w.ntx);
+    const int64_t x0 = (int64_t)tx * C::TX + lane * V;  // my first column
+    const int64_t y0 = (int64_t)ty * TY + warp * PY;    // my first row
+    const int col = HX + lane * V;                      // my first column in a slot
+    const int row0 = RYM + warp * PY;                   // my first row in a slot
+    const int64_t seg_planes = sg.zb - sg.za + 2 * R;
+    for (int64_t z = sg.za; z < sg.zb; ++z) {
+      // planes z-R .. z+R sit at ring positions n + (z - za) .. + 2R
+      const uint32_t q0 = n + (uint32_t)(z - sg.za);
+      bool ok = true;
+#pragma unroll
+      for (int k = 0; k < F; ++k) {
+        const uint32_t q = q0 + k;
+        if (!mbar_wait(&full[q % S], (q / S) & 1, w.wait_ns)) ok = false;
+      }
+      if (!ok) {
+        if (lane == 0) atomicCAS(w.err, 0, 3);
+        return;
+      }
+      TA acc[PY][V];
+      TA pr[PY][R];   // partial sums for the lane to the right
+      TA pl[PY][R];   // partial sums for the lane to the left
+      TA inl[PY][R];  // lane 0: contributions of the left halo columns
+      TA inr[PY][R];  // lane 31: contributions of the right halo columns
+      TA center[PY][V];
+#pragma unroll
+      for (int i = 0; i < PY; ++i) {
+#pragma unroll
+        for (int j = 0; j < V; ++j) acc[i][j] = center[i][j] = TA(0);
+#pragma unroll
+        for (int q = 0; q < R; ++q) pr[i][q] = pl[i][q] = inl[i][q] = inr[i][q] = TA(0);
+      }
+      const bool edge_lane = lane == 0 || lane == 31;
+#pragma unroll
+      for (int dz = -R; dz <= R; ++dz) {
+        const int ry = ry3<SH, R>(dz);  // folds to a constant once unrolled
+        if (ry < 0) continue;
+        const uint32_t q = q0 + (uint32_t)(dz + R);
+        const TS* slot = slots + (size_t)(q % S) * (C::SLOT_BYTES / sizeof(TS));
+        // y-strip register cache of this plane: rows -ry .. PY+ry-1
+        TA d[PY + 2 * RYM][V];
+        TA hv[PY + 2 * RYM][R];
+#pragma unroll
+        for (int k = -RYM; k < PY + RYM; ++k) {
+          if (k < -ry || k >= PY + ry) continue;
+          const TS* rowp = slot + (row0 + k) * XW + col;
+          load_slot_row<TS, V>(d[k + ry], rowp);
+          if (edge_lane) {
+#pragma unroll
+            for (int h = 0; h < R; ++h)
+              hv[k + ry][h] = to_acc(lane == 0 ? rowp[-1 - h] : rowp[V + h]);
+          }
+        }
+        if (dz == 0) {
+#pragma unroll
+          for (int i = 0; i < PY; ++i)
+#pragma unroll
+            for (int j = 0; j < V; ++j) center[i][j] = d[i + ry][j];
+        }
+#pragma unroll
+        for (int i = 0; i < PY; ++i) {
+#pragma unroll
+          for (int dy = -RYM; dy <= RYM; ++dy) {
+            if (dy < -ry || dy > ry || rx3<SH, R>(dz, dy) < 0) continue;
+#pragma unroll
+            for (int dx = -R; dx <= R; ++dx) {
+              if (!tap3<SH, R>(dz, dy, dx)) continue;
+              const TA c = cf.c[((dz + R) * F + (dy + R)) * F + (dx + R)];
+              const TA* src_row = d[i + dy + ry];
+#pragma unroll
+              for (int j = 0; j < V; ++j) {
+                const int t = j - dx;  // column that source column j feeds
+                if (t >= 0 && t < V) acc[i][t] = fma(c, src_row[j], acc[i][t]);
+                else if (t >= V) pr[i][t - V] = fma(c, src_row[j], pr[i][t - V]);
+                else pl[i][-1 - t] = fma(c, src_row[j], pl[i][-1 - t]);
+              }
+              if (edge_lane) {
+#pragma unroll
+                for (int h = 0; h < R; ++h) {
+                  const TA v = hv[i + dy + ry][h];
+                  const int tl = -1 - h - dx;  // lane 0: halo column -1-h feeds tl
+                  const int tr = V + h - dx;   // lane 31: halo column V+h feeds tr
+                  if (lane == 0) {
+                    if (tl >= 0 && tl < V) inl[i][tl] = fma(c, v, inl[i][tl]);
+                  } else {
+                    if (tr >= 0 && tr < V) inr[i][V - 1 - tr] = fma(c, v, inr[i][V - 1 - tr]);
+                  }
+                }
+              }
+            }
+          }
+        }
+      }
+      // systolic exchange: one hop right, one hop left (R <= V)
+#pragma unroll
+      for (int i = 0; i < PY; ++i) {
+#pragma unroll
+        for (int qq = 0; qq < R; ++qq) {
+          TA v = __shfl_up_sync(FULL, pr[i][qq], 1);
+          if (lane == 0) v = inl[i][qq];
+          acc[i][qq] += v;
+          TA u = __shfl_down_sync(FULL, pl[i][qq], 1);
+          if (lane == 31) u = inr[i][qq];
+          acc[i][V - 1 - qq] += u;
+        }
+      }
+      // planes whose last use this was: z - R (and the rest at segment end)
+      __syncwarp();
+      if (lane == 0) {
+        const uint32_t q = q0;
+        mbar_arrive(&empty[q % S]);
+        if (z == sg.zb - 1)
+          for (uint32_t k = 1; k < (uint32_t)F; ++k) mbar_arrive(&empty[(q0 + k) % S]);
+      }
+      // store PY rows x V columns
+      const bool zring = z < R || z >= nz - R;
+#pragma unroll
+      for (int i = 0; i < PY; ++i) {
+        const int64_t y = y0 + i;
+        if (y >= ny || x0 >= nx) continue;
+        TA o[V];
+#pragma unroll
+        for (int j = 0; j < V; ++j) {
+          o[j] = acc[i][j];
+          if (w.boundary == SSAM_BOUNDARY_COPY) {
+            const int64_t x = x0 + j;
+            if (zring || y < R || y >= ny - R || x < R || x >= nx - R) o[j] = center[i][j];
+          }
+        }
+        TS* outp = dst + z * nxy + y * nx + x0;
+        if (x0 + V <= nx && ((uintptr_t)outp % (V * sizeof(TS) >= 16 ? 16 : 8)) == 0) {
+          store_row<TS, V>(outp, o);
+        } else {
+#pragma unroll
+          for (int j = 0; j < V; ++j)
+            if (x0 + j < nx) outp[j] = from_acc<TS>(o[j]);
+        }
+      }
+    }
+    n += (uint32_t)seg_planes;
+  }
+}
+
+}  // namespace ssam
