@@ -25,6 +25,7 @@ int fail(int st, const std::string& msg) {
 }
 
 int fail_cuda(cudaError_t e, const char* what) {
+  cudaGetLastError();  // do not let a non-sticky error leak into the next call
   g_last_error = std::string(what) + ": " + cudaGetErrorName(e) + " (" +
                  cudaGetErrorString(e) + ")";
   return SSAM_ERR_CUDA;

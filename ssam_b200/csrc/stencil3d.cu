@@ -4,6 +4,7 @@
 #include <cudaTypedefs.h>
 #include <string.h>
 
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -60,6 +61,7 @@ struct Launch3D {
   const double* coef;  // (2R+1)^3, [dz][dy][dx]
   int boundary;
   cudaStream_t stream;
+  bool prepare_only;  // resolve attributes/occupancy/symbols, launch nothing
 };
 
 template <typename TS, int SH, int R, int PY, int NW, int S>
@@ -95,14 +97,27 @@ static int launch_3d(const Launch3D& a) {
   w.nz = a.nz;
   w.ntx = (int)((a.nx + C::TX - 1) / C::TX);
   w.nty = (int)((a.ny + C::TY - 1) / C::TY);
-  w.total = (int64_t)w.ntx * w.nty * a.nz;
+  // z chunk: minimise (rounds of items) x (chunk + 2R prologue planes)
   const int64_t grid_max = (int64_t)sms * bps;
-  w.per_cta = (w.total + grid_max - 1) / grid_max;
-  const int64_t grid = (w.total + w.per_cta - 1) / w.per_cta;
+  const int64_t ntiles = (int64_t)w.ntx * w.nty;
+  int64_t best = -1;
+  for (int zc : {8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512}) {
+    if (zc > 2 * a.nz && zc > 8) break;
+    const int64_t items = ntiles * ((a.nz + zc - 1) / zc);
+    const int64_t rounds = (items + grid_max - 1) / grid_max;
+    const int64_t cost = rounds * (std::min<int64_t>(zc, a.nz) + 2 * R);
+    if (best < 0 || cost < best) {
+      best = cost;
+      w.zc = zc;
+      w.items = items;
+    }
+  }
+  const int64_t grid = std::min(w.items, grid_max);
   w.boundary = a.boundary;
   w.wait_ns = 1000ull * 1000ull * 1000ull;  // 1 s per wait; healthy waits take microseconds
   int st = device_error_word(&w.err);
   if (st != SSAM_OK) return st;
+  if (a.prepare_only) return SSAM_OK;
 
   CUtensorMap map;
   memset(&map, 0, sizeof(map));
@@ -185,6 +200,24 @@ struct GraphEntry {
   int launches = 0;
 };
 
+// Captures run on a private stream: the caller's stream may be the legacy
+// default stream, which cannot be captured.  The graph is then launched on
+// the caller's stream.
+static cudaError_t capture_stream(cudaStream_t* out) {
+  thread_local int dev = -1;
+  thread_local cudaStream_t s = nullptr;
+  int d = 0;
+  cudaError_t e = cudaGetDevice(&d);
+  if (e != cudaSuccess) return e;
+  if (d != dev) {
+    e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return e;
+    dev = d;
+  }
+  *out = s;
+  return cudaSuccess;
+}
+
 static std::mutex g_graph_mu;
 static std::map<GraphKey, GraphEntry> g_graphs;
 static uint64_t g_graph_clock = 0;
@@ -196,7 +229,7 @@ static int enqueue_chain_3d(LaunchFn3D fn, const GraphKey& k, void* scratch,
   const void* in = k.src;
   for (int i = 0; i < k.steps; ++i) {
     void* out = ((k.steps - 1 - i) % 2 == 0) ? k.dst : scratch;
-    Launch3D a{in, out, k.nx, k.ny, k.nz, k.coef.data(), k.boundary, s};
+    Launch3D a{in, out, k.nx, k.ny, k.nz, k.coef.data(), k.boundary, s, false};
     int st = fn(a);
     if (st != SSAM_OK) return st;
     in = out;
@@ -248,12 +281,20 @@ int run_3d(const void* src, void* dst, int64_t nx, int64_t ny, int64_t nz, int d
     }
     GraphEntry e;
     e.device = dev;
+    // the scratch grid lives as long as the cached graph; make it usable from
+    // any stream the graph is later launched on
     int st = scratch_alloc(&e.scratch, bytes, stream);
     if (st != SSAM_OK) return st;
+    SSAM_CUDA_TRY(cudaStreamSynchronize(stream));
+    Launch3D prep{k.src, k.dst, k.nx, k.ny, k.nz, k.coef.data(), k.boundary, stream, true};
+    st = fn(prep);
+    if (st != SSAM_OK) return st;
+    cudaStream_t cs = nullptr;
+    SSAM_CUDA_TRY(capture_stream(&cs));
     cudaGraph_t graph = nullptr;
-    SSAM_CUDA_TRY(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-    st = enqueue_chain_3d(fn, k, e.scratch, stream);
-    cudaError_t ce = cudaStreamEndCapture(stream, &graph);
+    SSAM_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    st = enqueue_chain_3d(fn, k, e.scratch, cs);
+    cudaError_t ce = cudaStreamEndCapture(cs, &graph);
     if (st != SSAM_OK || ce != cudaSuccess) {
       if (graph) cudaGraphDestroy(graph);
       scratch_free(e.scratch, stream);

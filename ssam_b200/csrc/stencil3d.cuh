@@ -17,9 +17,10 @@
 //     columns instead);
 //   * z-neighbours are read from the slots of the adjacent planes (shared
 //     memory between warps, as in the reference);
-//   * work is split evenly over a persistent grid as contiguous runs of
-//     (column tile, plane) pairs, so the grid is sized to the SM count and no
-//     tile restarts more than once;
+//   * work items are (z chunk, column tile) pairs taken chunk-major with a
+//     stride of the grid size by a persistent grid sized to the SMs, so that
+//     neighbouring tiles of the same z chunk run at the same time and share
+//     their halos through L2;
 //   * every mbarrier wait is bounded (%globaltimer): on expiry the kernel
 //     records an error code, the producer drains its own copies in flight
 //     (again bounded), and the CTA returns.
@@ -85,8 +86,8 @@ struct Stencil3DCfg {
 struct Work3D {
   int64_t nx, ny, nz;
   int ntx, nty;          // column tiles
-  int64_t total;         // ntx*nty*nz (tile, plane) pairs
-  int64_t per_cta;       // contiguous pairs per CTA
+  int zc;                // planes per work item (z chunk)
+  int64_t items;         // ntx*nty*ceil(nz/zc) (chunk, tile) work items
   int boundary;
   int use_tma;
   unsigned long long wait_ns;
@@ -188,23 +189,24 @@ __device__ __forceinline__ void store_row(TS* p, const TA (&o)[V]) {
   }
 }
 
-// Segment = run of consecutive planes [za, zb) of one column tile.
+// Work item `it` = (z chunk, column tile), chunk-major.  CTAs take items
+// it = blockIdx.x + k*gridDim.x, so at any moment the grid works on a band
+// of consecutive items -- the same z chunk of neighbouring tiles -- and the
+// halo rows and columns that neighbouring tiles share are served by L2.
 struct Seg3D {
   int64_t tile, za, zb;
 };
-__device__ __forceinline__ bool next_seg(int64_t& pos, int64_t end, int64_t nz, Seg3D& s) {
-  if (pos >= end) return false;
-  s.tile = pos / nz;
-  s.za = pos % nz;
-  const int64_t tile_end = (s.tile + 1) * nz;
-  const int64_t stop = end < tile_end ? end : tile_end;
-  s.zb = s.za + (stop - pos);
-  pos = stop;
-  return true;
+__device__ __forceinline__ Seg3D item_seg(int64_t it, const Work3D& w) {
+  const int64_t ntiles = (int64_t)w.ntx * w.nty;
+  Seg3D s;
+  s.tile = it % ntiles;
+  s.za = (it / ntiles) * w.zc;
+  s.zb = s.za + w.zc < w.nz ? s.za + w.zc : w.nz;
+  return s;
 }
 
 template <typename TS, int SH, int R, int PY, int NW, int S>
-__global__ void __launch_bounds__(32 * (NW + 1), 1)
+__global__ void __launch_bounds__(32 * (NW + 1), 2)
 stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__ src,
                  TS* __restrict__ dst, Work3D w,
                  CoefBlock<typename Traits<TS>::TA,
@@ -232,17 +234,14 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
   }
   __syncthreads();
 
-  const int64_t begin = (int64_t)blockIdx.x * w.per_cta;
-  const int64_t end = begin + w.per_cta < w.total ? begin + w.per_cta : w.total;
   const int64_t nx = w.nx, ny = w.ny, nz = w.nz, nxy = nx * ny;
 
   if (warp == NW) {
     // ------------------------------------------------------ producer warp
     uint32_t n = 0;  // planes issued so far (ring position)
     bool ok = true;
-    int64_t pos = begin;
-    Seg3D sg;
-    while (ok && next_seg(pos, end, nz, sg)) {
+    for (int64_t it = blockIdx.x; ok && it < w.items; it += gridDim.x) {
+      const Seg3D sg = item_seg(it, w);
       const int tx = (int)(sg.tile % w.ntx), ty = (int)(sg.tile / w.ntx);
       const int gx = tx * C::TX - HX, gy = ty * TY - RYM;
       for (int64_t p = sg.za - R; p < sg.zb + R; ++p, ++n) {
@@ -285,9 +284,8 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
 
   // --------------------------------------------------------- consumer warps
   uint32_t n = 0;  // ring position of the segment's first plane
-  int64_t pos = begin;
-  Seg3D sg;
-  while (next_seg(pos, end, nz, sg)) {
+  for (int64_t it = blockIdx.x; it < w.items; it += gridDim.x) {
+    const Seg3D sg = item_seg(it, w);
     const int tx = (int)(sg.tile % w.ntx), ty = (int)(sg.tile / w.ntx);
     const int64_t x0 = (int64_t)tx * C::TX + lane * V;  // my first column
     const int64_t y0 = (int64_t)ty * TY + warp * PY;    // my first row
