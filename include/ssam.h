@@ -165,6 +165,31 @@ SSAM_API int ssam_stencil2d_host(const void* h_src, void* h_dst, int64_t width,
                                  int radius, const double* coeffs, int steps,
                                  int boundary, void* stream);
 
+/* Largest scratch grid, in bytes (pitch * height * element size), that
+ * ssam_stencil2d_noalloc can hold. */
+#define SSAM_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+
+/*
+ * ssam_stencil2d for callers that cannot allocate device memory.  No
+ * counterpart in the reference (it has no library interface at all).
+ *
+ * Callers inside a fixed device-memory budget, or hosts that forbid
+ * allocation after start-up, cannot let ssam_stencil2d take its multi-step
+ * scratch grid from a memory pool.  This entry point computes the same steps
+ * with the same kernels, but keeps that scratch grid in a library-owned
+ * device array of SSAM_NOALLOC_SCRATCH_BYTES that every GPU loading the
+ * library holds until exit; it calls no allocator.  A run that needs scratch
+ * (more than one launch in the chain) and a grid larger than the array
+ * fails with SSAM_ERR_INVALID.  The array's device address is looked up on
+ * the first call on each device (make that call before any stream capture).
+ * All calls share the array: calls that overlap on the GPU race, so callers
+ * serialise them.
+ */
+SSAM_API int ssam_stencil2d_noalloc(const void* src, void* dst, int64_t width,
+                                    int64_t height, int64_t pitch, int dtype, int shape,
+                                    int radius, const double* coeffs, int steps,
+                                    int boundary, void* stream);
+
 /*
  * Generic 2D correlation with an fw x fh weight matrix (1 <= fw, fh <= 28):
  *   dst(y, x) = sum_{n<fh, m<fw} weight[n*fw + m] * src(y + n - fh/2, x + m - fw/2)

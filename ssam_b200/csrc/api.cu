@@ -127,7 +127,7 @@ static bool grids_overlap(const void* a, const void* b, int64_t w, int64_t h,
   return pa < pb + len && pb < pa + len;
 }
 
-static int check_grid2d(const void* src, const void* dst, int64_t w, int64_t h,
+int check_grid2d(const void* src, const void* dst, int64_t w, int64_t h,
                         int64_t pitch, int dtype, int boundary) {
   if (!src || !dst) return fail(SSAM_ERR_INVALID, "src and dst must be device pointers");
   if (w < 1 || h < 1) return fail(SSAM_ERR_INVALID, "width and height must be >= 1");
@@ -143,14 +143,8 @@ static int check_grid2d(const void* src, const void* dst, int64_t w, int64_t h,
 
 // ------------------------------------------------------------- 2D planning --
 
-struct Plan2D {
-  Key2D key;
-  const Kernel2DInfo* info;
-  int warps;
-};
-
 // Chooses a compiled kernel for one launch of `t` fused steps.
-static int pick_2d(int dtype, int rl, int rr, int rt, int rb, int star, int t,
+int pick_2d(int dtype, int rl, int rr, int rt, int rb, int star, int t,
                    int64_t w, int64_t h, Plan2D* out) {
   TuneChoice c;
   if (!tune_lookup_2d(dtype, rl, rr, rt, rb, star, t, w, h, &c)) {
@@ -178,7 +172,7 @@ static int pick_2d(int dtype, int rl, int rr, int rt, int rb, int star, int t,
 }
 
 // A kernel fusing `t` steps is compiled for this stencil (any P).
-static bool have_depth_2d(int dtype, int rl, int rr, int rt, int rb, int star, int t) {
+bool have_depth_2d(int dtype, int rl, int rr, int rt, int rb, int star, int t) {
   struct Acc { int t; bool found; } acc{t, false};
   list_2d(dtype, rl, rr, rt, rb, star,
           [](const Key2D& k, const Kernel2DInfo&, void* u) {
@@ -236,7 +230,7 @@ static int run_2d(const void* src, void* dst, int64_t w, int64_t h, int64_t pitc
 
 // Dense (2r+1)^2 coefficient matrix from the ABI's STAR or BOX layout, with
 // the argument checks shared by the device- and host-buffer entry points.
-static int stencil_matrix(int shape, int radius, const double* coeffs, int steps,
+int stencil_matrix(int shape, int radius, const double* coeffs, int steps,
                           int boundary, std::vector<double>* out) {
   if (shape != SSAM_STAR && shape != SSAM_BOX)
     return fail(SSAM_ERR_INVALID, "shape must be SSAM_STAR or SSAM_BOX");

@@ -152,6 +152,13 @@ struct Kernel2DInfo {
   int vec;           // elements per thread along x
 };
 
+// A chosen kernel and block size for one launch.
+struct Plan2D {
+  Key2D key;
+  const Kernel2DInfo* info;
+  int warps;
+};
+
 void register_2d(const Key2D& k, const Kernel2DInfo& info);
 const Kernel2DInfo* find_2d(const Key2D& k);
 // All registered kernels matching dtype/radii/shape (any P, T).
