@@ -203,6 +203,38 @@ SSAM_API int ssam_conv2d(const void* src, void* dst, int64_t width, int64_t pitc
                 int64_t height, int dtype, const double* weight, int fw, int fh,
                 int boundary, void* stream);
 
+/* -------------------------------------------------------------- autotuner */
+
+/* What the autotuner chose for one stencil and grid size. */
+typedef struct ssam_tune_report {
+  int rows_per_thread;    /* P: output rows a thread keeps in registers */
+  int warps_per_block;    /* warps per thread block */
+  int columns_per_thread; /* V: columns a thread owns; warp strip = 32*V */
+  int fused_steps;        /* temporal depth: steps fused per launch */
+  int candidates;         /* kernel configurations timed */
+  double ms_per_step;     /* best measured time per step (ms) */
+} ssam_tune_report;
+
+/*
+ * Times every compiled configuration of this stencil -- outputs per thread,
+ * strip width, warps per block and temporal depth -- on the caller's buffers
+ * (dst is overwritten) and stores the fastest for the grid's size class
+ * (log2 of width and height); later ssam_stencil2d / _host / _noalloc calls
+ * on grids of that class use it.  The reference hand-picks these constants
+ * per GPU (PROCESS_DATA_COUNT, BLOCK_SIZE, ITERATIVE_COUNT chosen with
+ * IsTeslaV100(), tmp3d7pt-v2.cu:341-387); this replaces that choice.
+ * Synchronous: returns after the timing runs.  `report` may be NULL.
+ */
+SSAM_API int ssam_autotune_stencil2d(const void* src, void* dst, int64_t width,
+                                     int64_t height, int64_t pitch, int dtype, int shape,
+                                     int radius, const double* coeffs, int steps,
+                                     int boundary, void* stream, ssam_tune_report* report);
+
+/* Persist / restore / forget the measured choices (a small text file). */
+SSAM_API int ssam_autotune_save(const char* path);
+SSAM_API int ssam_autotune_load(const char* path);
+SSAM_API int ssam_autotune_clear(void);
+
 /* ------------------------------------------------------------ 3D stencils */
 
 /*

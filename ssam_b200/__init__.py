@@ -59,6 +59,12 @@ def _declare(lib):
     lib.ssam_device_status.restype = _int
     lib.ssam_device_status.argtypes = [_vp]
     lib.ssam_trim_scratch.restype = _int
+    lib.ssam_autotune_stencil2d.restype = _int
+    lib.ssam_autotune_stencil2d.argtypes = lib.ssam_stencil2d.argtypes + [_vp]
+    for name in ("ssam_autotune_save", "ssam_autotune_load"):
+        getattr(lib, name).restype = _int
+        getattr(lib, name).argtypes = [ctypes.c_char_p]
+    lib.ssam_autotune_clear.restype = _int
     lib.ssam_conv2d.restype = _int
     lib.ssam_conv2d.argtypes = [_vp, _vp, _i64, _i64, _i64, _int, _dp, _int, _int,
                                 _int, _vp]
@@ -221,6 +227,42 @@ def device_status(stream=None) -> None:
     import torch
     s = stream if stream is not None else torch.cuda.current_stream()
     _check(lib().ssam_device_status(ctypes.c_void_p(s.cuda_stream)))
+
+
+class TuneReport(ctypes.Structure):
+    """``ssam_tune_report``."""
+    _fields_ = [("rows_per_thread", ctypes.c_int), ("warps_per_block", ctypes.c_int),
+                ("columns_per_thread", ctypes.c_int), ("fused_steps", ctypes.c_int),
+                ("candidates", ctypes.c_int), ("ms_per_step", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def autotune_stencil2d(src, coeffs, radius: int, shape: int = STAR, steps: int = 1,
+                       boundary: str = "zero", dst=None, stream=None) -> dict:
+    """Measure every compiled configuration on ``src`` (``dst`` is scratch)
+    and keep the fastest for this grid size class (``ssam_autotune_stencil2d``)."""
+    dst = _grid2d(src, dst)
+    h, w = src.shape
+    rep = TuneReport()
+    _check(lib().ssam_autotune_stencil2d(src.data_ptr(), dst.data_ptr(), w, h, src.stride(0),
+                                         _dtype_code(src), shape, radius, _doubles(coeffs),
+                                         steps, BOUNDARY[boundary], _stream_ptr(src, stream),
+                                         ctypes.byref(rep)))
+    return rep.as_dict()
+
+
+def autotune_save(path: str) -> None:
+    _check(lib().ssam_autotune_save(path.encode()))
+
+
+def autotune_load(path: str) -> None:
+    _check(lib().ssam_autotune_load(path.encode()))
+
+
+def autotune_clear() -> None:
+    _check(lib().ssam_autotune_clear())
 
 
 def star_coeffs_from_matrix(m) -> list[float]:

@@ -35,30 +35,40 @@ DTYPES = {"f32": "float", "f64": "double", "bf16": "__nv_bfloat16", "f16": "__ha
 
 
 def instances():
-    """(dtype, star, rl, rr, P, T) of every compiled 2D kernel."""
+    """(dtype, star, rl, rr, P, T, V) of every compiled 2D kernel.
+
+    V is the number of columns a thread owns (the warp strip is 32*V
+    columns): 4 (16 bytes) for FP32, 4 (32 bytes) for FP64, 8 (16 bytes) for
+    the 16-bit types by default; FP32/FP64 also get V = 8 for the single-step
+    stencils, which halves the halo lanes of the wide (r > 4) stencils and
+    gives the autotuner a second strip width.
+    """
     out = []
     for dt in DTYPES:
         wide = dt in ("f32", "f64")
-        # star r = 1..6 (5/9/13/17/21/25-pt)
-        for r in range(1, 7):
-            for p in (4, 8, 16):
-                out.append((dt, 1, r, r, p, 1))
-        # box r = 1..5 (9/25/49/81/121-pt; conv F = 3..11)
-        for r in range(1, 6):
-            for p in (4, 8, 16):
-                out.append((dt, 0, r, r, p, 1))
+        v0 = 4 if wide else 8
+        vs = (v0, 8) if wide else (v0,)
+        # star r = 1..6 (5/9/13/17/21/25-pt) and box r = 1..5
+        # (9/25/49/81/121-pt; conv F = 3..11)
+        for star, rmax in ((1, 6), (0, 5)):
+            for r in range(1, rmax + 1):
+                for v in vs:
+                    for p in ((4, 8, 16) if v == v0 else (4, 8)):
+                        out.append((dt, star, r, r, p, 1, v))
         # temporal blocking for the bandwidth-bound radii
         for star in (1, 0):
             for r, ts in ((1, (2, 4, 8)), (2, (2, 4))):
                 for t in ts:
-                    out.append((dt, star, r, r, 8, t))
+                    out.append((dt, star, r, r, 8, t, v0))
         # every other square conv size up to 28 (even F has rl = rr + 1)
         if wide:
             for f in range(1, 29):
                 rl, rr = f // 2, f - 1 - f // 2
                 if f % 2 == 1 and 1 <= rl <= 5:
                     continue
-                out.append((dt, 0, rl, rr, 4, 1))
+                out.append((dt, 0, rl, rr, 4, 1, v0))
+                if rl > 4:
+                    out.append((dt, 0, rl, rr, 4, 1, 8))
     return out
 
 
@@ -74,11 +84,11 @@ def _gen_units(chunk: int = 6):
             name = f"inst2d_{dt}_{c // chunk:02d}.cu"
             lines = ["// generated by ssam_b200/build.py -- do not edit",
                      '#include "../../csrc/stencil2d.cuh"', "namespace ssam {"]
-            for (_, star, rl, rr, p, t) in part:
-                tag = f"{'s' if star else 'b'}_{rl}_{rr}_{p}_{t}"
+            for (_, star, rl, rr, p, t, v) in part:
+                tag = f"{'s' if star else 'b'}_{rl}_{rr}_{p}_{t}_{v}"
                 lines.append(
                     f"static Register2D<{DTYPES[dt]}, {rl}, {rr}, {rl}, {rr}, "
-                    f"{'true' if star else 'false'}, {p}, {t}> reg_{tag};")
+                    f"{'true' if star else 'false'}, {p}, {t}, {v}> reg_{tag};")
             lines.append("}  // namespace ssam")
             text = "\n".join(lines) + "\n"
             path = os.path.join(BUILD, "gen", name)

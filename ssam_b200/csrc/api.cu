@@ -83,9 +83,9 @@ void scratch_free(void* p, cudaStream_t s) {
 // ---------------------------------------------------------------- registry --
 
 bool Key2D::operator<(const Key2D& o) const {
-  const int a[8] = {dtype, rl, rr, rt, rb, star, p, t};
-  const int b[8] = {o.dtype, o.rl, o.rr, o.rt, o.rb, o.star, o.p, o.t};
-  return std::lexicographical_compare(a, a + 8, b, b + 8);
+  const int a[9] = {dtype, rl, rr, rt, rb, star, p, t, v};
+  const int b[9] = {o.dtype, o.rl, o.rr, o.rt, o.rb, o.star, o.p, o.t, o.v};
+  return std::lexicographical_compare(a, a + 9, b, b + 9);
 }
 bool Key2D::operator==(const Key2D& o) const { return !(*this < o) && !(o < *this); }
 
@@ -150,13 +150,16 @@ int pick_2d(int dtype, int rl, int rr, int rt, int rb, int star, int t,
   if (!tune_lookup_2d(dtype, rl, rr, rt, rb, star, t, w, h, &c)) {
     c = tune_default_2d(dtype, rl, rr, rt, rb, star, t);
   }
-  Key2D k{dtype, rl, rr, rt, rb, star, c.p, t};
+  Key2D k{dtype, rl, rr, rt, rb, star, c.p, t, c.v};
   const Kernel2DInfo* info = find_2d(k);
-  if (!info) {
-    // any compiled P for this shape and depth, smallest first
+  // otherwise any compiled (P, V) for this shape and depth, default width first
+  const int vdef = dtype == SSAM_BF16 || dtype == SSAM_F16 ? 8 : 4;
+  for (int v : {vdef, 4, 8, 2, 16}) {
     for (int p : {4, 8, 16, 2, 1}) {
+      if (info) break;
       k.p = p;
-      if ((info = find_2d(k))) break;
+      k.v = v;
+      info = find_2d(k);
     }
   }
   if (!info)

@@ -10,6 +10,7 @@ namespace ssam {
 struct TuneChoice {
   int p;      // output rows per thread (template P)
   int warps;  // warps per block
+  int v;      // columns per thread (template V; warp strip = 32*V columns)
 };
 
 // Measured choice for this stencil, fused depth and grid size, if any.

@@ -42,8 +42,8 @@ void scratch_free(void* p, cudaStream_t s);
 
 // ------------------------------------------------------------ dtype traits --
 
-// TA = accumulation type, V = elements a thread owns along x (one or two
-// 16-byte chunks).
+// TA = accumulation type, V = default number of columns a thread owns along
+// x (16 or 32 bytes); the 2D kernels are also compiled for other widths.
 template <typename TS> struct Traits;
 template <> struct Traits<float> {
   using TA = float;
@@ -126,9 +126,9 @@ struct CoefBlock {
 // ---------------------------------------------------------- kernel registry --
 
 // One compiled 2D stencil kernel: radii left/right/top/bottom, tap pattern,
-// outputs per thread along y (P) and fused time steps (T).
+// outputs per thread along y (P), fused time steps (T), columns per thread (V).
 struct Key2D {
-  int dtype, rl, rr, rt, rb, star, p, t;
+  int dtype, rl, rr, rt, rb, star, p, t, v;
   bool operator<(const Key2D& o) const;
   bool operator==(const Key2D& o) const;
 };

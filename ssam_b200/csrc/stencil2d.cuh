@@ -29,17 +29,18 @@
 //
 // Template parameters: TS storage type, RL/RR/RT/RB reach to the left, right,
 // top (smaller y) and bottom, STAR (only the centre row and column are
-// non-zero), P output rows per thread, T fused steps.
+// non-zero), P output rows per thread, T fused steps, V columns per thread
+// (the warp strip is 32*V columns wide).
 #pragma once
 
 #include "ssam_internal.cuh"
 
 namespace ssam {
 
-template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int P, int T>
+template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int P, int T, int V_>
 struct Stencil2DCfg {
   using TA = typename Traits<TS>::TA;
-  static constexpr int V = Traits<TS>::V;
+  static constexpr int V = V_;
   static constexpr int FW = RL + RR + 1;
   static constexpr int FH = RT + RB + 1;
   static constexpr int NC = FW * FH;
@@ -49,6 +50,7 @@ struct Stencil2DCfg {
   static constexpr int OUT_COLS = OUT_LANES * V;
   static constexpr int ROWS = P + (RT + RB) * T;
   static_assert(OUT_LANES >= 2, "radius too large for one warp strip");
+  static_assert((V * sizeof(TS)) % 16 == 0, "a thread owns whole 16-byte chunks");
 };
 
 // Boundary rule applied to a value of the register window that sits at
@@ -92,14 +94,14 @@ __device__ __forceinline__ void store_row_edge(TS* __restrict__ row, int64_t x0,
     if (x0 + j < W) row[x0 + j] = from_acc<TS>(d[j]);
 }
 
-template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int P, int T>
+template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int P, int T, int V_>
 __global__ void __launch_bounds__(256)
 stencil2d_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int64_t W,
                  int64_t H, int64_t pitch, int64_t y_begin, int64_t y_end, int bnd,
                  int vec_ok,
                  CoefBlock<typename Traits<TS>::TA,
-                           Stencil2DCfg<TS, RL, RR, RT, RB, STAR, P, T>::NC> cf) {
-  using C = Stencil2DCfg<TS, RL, RR, RT, RB, STAR, P, T>;
+                           Stencil2DCfg<TS, RL, RR, RT, RB, STAR, P, T, V_>::NC> cf) {
+  using C = Stencil2DCfg<TS, RL, RR, RT, RB, STAR, P, T, V_>;
   using TA = typename C::TA;
   constexpr int V = C::V;
   constexpr int FW = C::FW;
@@ -302,9 +304,9 @@ stencil2d_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int64_t W,
   }
 }
 
-template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int P, int T>
+template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int P, int T, int V_>
 cudaError_t launch_stencil2d(const Launch2D& a) {
-  using C = Stencil2DCfg<TS, RL, RR, RT, RB, STAR, P, T>;
+  using C = Stencil2DCfg<TS, RL, RR, RT, RB, STAR, P, T, V_>;
   using TA = typename C::TA;
   CoefBlock<TA, C::NC> cf;
   for (int k = 0; k < C::NC; ++k) cf.c[k] = (TA)a.coef[k];
@@ -314,21 +316,21 @@ cudaError_t launch_stencil2d(const Launch2D& a) {
   dim3 grid((unsigned)((warps_x + nw - 1) / nw), (unsigned)(nby < 65535 ? nby : 65535));
   const int vec_ok = ((uintptr_t)a.src % 16 == 0) && ((uintptr_t)a.dst % 16 == 0) &&
                      (a.pitch % C::V == 0);
-  stencil2d_kernel<TS, RL, RR, RT, RB, STAR, P, T><<<grid, 32 * nw, 0, a.stream>>>(
+  stencil2d_kernel<TS, RL, RR, RT, RB, STAR, P, T, V_><<<grid, 32 * nw, 0, a.stream>>>(
       (const TS*)a.src, (TS*)a.dst, a.width, a.height, a.pitch, a.y_begin, a.y_end,
       a.boundary, vec_ok, cf);
   count_launch();
   return cudaGetLastError();
 }
 
-template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int P, int T>
+template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int P, int T, int V_>
 struct Register2D {
   Register2D() {
     Kernel2DInfo info;
-    info.launch = &launch_stencil2d<TS, RL, RR, RT, RB, STAR, P, T>;
-    info.func = (const void*)&stencil2d_kernel<TS, RL, RR, RT, RB, STAR, P, T>;
-    info.vec = Traits<TS>::V;
-    register_2d(Key2D{Traits<TS>::DT, RL, RR, RT, RB, STAR ? 1 : 0, P, T}, info);
+    info.launch = &launch_stencil2d<TS, RL, RR, RT, RB, STAR, P, T, V_>;
+    info.func = (const void*)&stencil2d_kernel<TS, RL, RR, RT, RB, STAR, P, T, V_>;
+    info.vec = V_;
+    register_2d(Key2D{Traits<TS>::DT, RL, RR, RT, RB, STAR ? 1 : 0, P, T, V_}, info);
   }
 };
 

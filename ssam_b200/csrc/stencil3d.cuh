@@ -292,6 +292,9 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
     const int col = HX + lane * V;                      // my first column in a slot
     const int row0 = RYM + warp * PY;                   // my first row in a slot
     const int64_t seg_planes = sg.zb - sg.za + 2 * R;
+    // does my strip touch the x/y ring that COPY keeps?
+    const bool ring_xy = w.boundary == SSAM_BOUNDARY_COPY &&
+                         (x0 < R || x0 + V > nx - R || y0 < R || y0 + PY > ny - R);
     for (int64_t z = sg.za; z < sg.zb; ++z) {
       // planes z-R .. z+R sit at ring positions n + (z - za) .. + 2R
       const uint32_t q0 = n + (uint32_t)(z - sg.za);
@@ -318,7 +321,6 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
 #pragma unroll
         for (int q = 0; q < R; ++q) pr[i][q] = pl[i][q] = inl[i][q] = inr[i][q] = TA(0);
       }
-      const bool edge_lane = lane == 0 || lane == 31;
 #pragma unroll
       for (int dz = -R; dz <= R; ++dz) {
         const int ry = ry3<SH, R>(dz);  // folds to a constant once unrolled
@@ -333,11 +335,12 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
           if (k < -ry || k >= PY + ry) continue;
           const TS* rowp = slot + (row0 + k) * XW + col;
           load_slot_row<TS, V>(d[k + ry], rowp);
-          if (edge_lane) {
+          // every lane reads the columns beyond its strip on the side that
+          // matters to lane 0 / lane 31; only those two lanes use the result
+          // (no divergent branch: the warp issues the load once either way)
 #pragma unroll
-            for (int h = 0; h < R; ++h)
-              hv[k + ry][h] = to_acc(lane == 0 ? rowp[-1 - h] : rowp[V + h]);
-          }
+          for (int h = 0; h < R; ++h)
+            hv[k + ry][h] = to_acc(rowp[lane == 0 ? -1 - h : V + h]);
         }
         if (dz == 0) {
 #pragma unroll
@@ -362,18 +365,13 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
                 else if (t >= V) pr[i][t - V] = fma(c, src_row[j], pr[i][t - V]);
                 else pl[i][-1 - t] = fma(c, src_row[j], pl[i][-1 - t]);
               }
-              if (edge_lane) {
 #pragma unroll
-                for (int h = 0; h < R; ++h) {
-                  const TA v = hv[i + dy + ry][h];
-                  const int tl = -1 - h - dx;  // lane 0: halo column -1-h feeds tl
-                  const int tr = V + h - dx;   // lane 31: halo column V+h feeds tr
-                  if (lane == 0) {
-                    if (tl >= 0 && tl < V) inl[i][tl] = fma(c, v, inl[i][tl]);
-                  } else {
-                    if (tr >= 0 && tr < V) inr[i][V - 1 - tr] = fma(c, v, inr[i][V - 1 - tr]);
-                  }
-                }
+              for (int h = 0; h < R; ++h) {
+                const TA v = hv[i + dy + ry][h];
+                const int tl = -1 - h - dx;  // as lane 0: halo column -1-h feeds tl
+                const int tr = V + h - dx;   // as lane 31: halo column V+h feeds tr
+                if (tl >= 0 && tl < V) inl[i][tl] = fma(c, v, inl[i][tl]);
+                if (tr >= 0 && tr < V) inr[i][V - 1 - tr] = fma(c, v, inr[i][V - 1 - tr]);
               }
             }
           }
@@ -401,7 +399,8 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
           for (uint32_t k = 1; k < (uint32_t)F; ++k) mbar_arrive(&empty[(q0 + k) % S]);
       }
       // store PY rows x V columns
-      const bool zring = z < R || z >= nz - R;
+      const bool zring = w.boundary == SSAM_BOUNDARY_COPY && (z < R || z >= nz - R);
+      const bool any_ring = ring_xy || zring;
 #pragma unroll
       for (int i = 0; i < PY; ++i) {
         const int64_t y = y0 + i;
@@ -410,7 +409,7 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
 #pragma unroll
         for (int j = 0; j < V; ++j) {
           o[j] = acc[i][j];
-          if (w.boundary == SSAM_BOUNDARY_COPY) {
+          if (any_ring) {
             const int64_t x = x0 + j;
             if (zring || y < R || y >= ny - R || x < R || x >= nx - R) o[j] = center[i][j];
           }

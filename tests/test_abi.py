@@ -69,3 +69,28 @@ def test_python_front_end_refuses_host_tensors():
     import torch
     with pytest.raises(ValueError):
         S.stencil2d(torch.zeros(8, 8), [0.2] * 5, 1)
+
+
+def test_autotune_cache_file_roundtrip(tmp_path):
+    """The tuning cache persists as text and rejects malformed files (no GPU)."""
+    lib = S.lib()
+    S.autotune_clear()
+    p = tmp_path / "tune.txt"
+    S.autotune_save(str(p))
+    assert p.read_text().startswith("# ssam_b200 autotune cache")
+    p.write_text("# ssam_b200 autotune cache v1\n"
+                 "choice 0 1 1 1 1 0 1 13 13 8 4 4\n"
+                 "depth 0 1 1 1 1 0 13 13 4\n")
+    S.autotune_load(str(p))
+    q = tmp_path / "again.txt"
+    S.autotune_save(str(q))
+    assert "choice 0 1 1 1 1 0 1 13 13 8 4 4" in q.read_text()
+    assert "depth 0 1 1 1 1 0 13 13 4" in q.read_text()
+    bad = tmp_path / "bad.txt"
+    bad.write_text("choice 1 2 3\n")
+    with pytest.raises(S.SsamError):
+        S.autotune_load(str(bad))
+    with pytest.raises(S.SsamError):
+        S.autotune_load(str(tmp_path / "missing.txt"))
+    S.autotune_clear()
+    assert lib.ssam_autotune_clear() == 0
