@@ -63,6 +63,13 @@ def workloads():
                                                   steps=100, boundary="copy")
             w[f"{gold}_{dt}_512"] = dict(kind="3d", gold=gold, r=r, dtype=dt, n=512,
                                          steps=1, boundary="copy")
+    # batches of 256 uneven grids (sides log-uniform in [64, 2048]), 50 steps
+    for dt in ("f32", "bf16", "f64"):
+        w[f"batched256_star1_{dt}_50steps"] = dict(kind="batched", shape="star", r=1, dtype=dt,
+                                                   ngrids=256, steps=50, boundary="copy",
+                                                   coeffs=[0.2] * 5, n=2048)
+        w[f"batched256_box2_{dt}_50steps"] = dict(kind="batched", shape="box", r=2, dtype=dt,
+                                                  ngrids=256, steps=50, boundary="copy", n=2048)
     return w
 
 
@@ -71,6 +78,8 @@ DEFAULT = "box1_f32_8192"
 
 def taps(spec) -> int:
     r = spec["r"]
+    if spec["kind"] == "batched":
+        return 4 * r + 1 if spec["shape"] == "star" else (2 * r + 1) ** 2
     if spec["kind"] == "3d":
         return {"j3d7pt": 7, "j3d13pt": 13, "poisson": 19}[spec["gold"]]
     if spec["kind"] == "star":
@@ -277,12 +286,18 @@ def run_reference(args, spec, name):
     rates = []
     sample = cores = None
     for i in range(n_steps):
-        rate, sample, cores = cpu_reference_rate(spec, budget, seed=i)
+        if spec["kind"] == "batched":
+            cb = batched_cpu_baseline(spec, batch_sides(spec), budget)
+            rate, sample, cores = cb["value"], cb["sample"], cb["cores"]
+        else:
+            rate, sample, cores = cpu_reference_rate(spec, budget, seed=i)
         if i >= args.warmup:
             rates.append(rate)
     value = statistics.median(rates) if rates else None
     nd = 3 if spec["kind"] == "3d" else 2
     cells = spec["n"] ** nd * spec["steps"]
+    if spec["kind"] == "batched":
+        cells = int(sum(int(h) * int(w_) for h, w_ in batch_sides(spec))) * spec["steps"]
     line = {
         "impl": "reference", "metric": "GCells/s", "value": value, "unit": "GCells/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -301,6 +316,143 @@ def run_reference(args, spec, name):
 
 
 # ------------------------------------------------------------------ our arm --
+
+def batch_sides(spec, seed=256):
+    g = np.random.Generator(np.random.PCG64(seed))
+    return np.exp(g.uniform(np.log(64), np.log(2048), size=(spec["ngrids"], 2))).astype(int)
+
+
+def run_batched(args, spec, name):
+    """256 uneven grids, `steps` steps each: one persistent launch per call
+    (value) against one launch chain per grid (reported beside it)."""
+    import torch
+    import ssam_b200 as S
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    tdt = {"f32": torch.float32, "f64": torch.float64, "bf16": torch.bfloat16}[spec["dtype"]]
+    sides = batch_sides(spec)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(2000 + rank)
+    srcs = [torch.rand(int(h), int(w_), device=dev, generator=gen).to(tdt) for h, w_ in sides]
+    dsts = [torch.empty_like(x) for x in srcs]
+    c = coefficients(spec)
+    r = spec["r"]
+    shape = S.STAR if spec["shape"] == "star" else S.BOX
+    stream = torch.cuda.current_stream(dev)
+    cells = int(sum(int(h) * int(w_) for h, w_ in sides))
+
+    def call(persistent):
+        S.stencil2d_batched(srcs, c, r, shape, spec["steps"], spec["boundary"], dsts=dsts,
+                            persistent=persistent, stream=stream)
+
+    def timed(persistent, k):
+        for _ in range(args.warmup):
+            call(persistent)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        l0 = S.lib().ssam_kernel_launches()
+        a.record(stream)
+        for _ in range(k):
+            call(persistent)
+        b.record(stream)
+        l1 = S.lib().ssam_kernel_launches()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / k, (l1 - l0) // k
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms, launches = timed(True, args.steps)
+    clk = clocks.stop()
+    ms_pg, launches_pg = timed(False, max(1, min(args.steps, 3)))
+    value = cells * spec["steps"] * world / (ms / 1e3) / 1e9
+    es = elem_size(spec["dtype"])
+    # phases of the persistent run: fused depth 4 (r=1) / 2 (r=2), rest single steps
+    deep = 4 if r == 1 else (2 if r == 2 else 1)
+    phases = spec["steps"] // deep + spec["steps"] % deep
+    alg_bytes = 2 * cells * es * phases
+    peak, peak_kind = load_peaks()
+    achieved = alg_bytes / (ms / 1e3) / 1e9
+    # end to end: every grid copied in from pinned host memory and back, per call
+    hs = [x.cpu().pin_memory() for x in srcs]
+    ho = [torch.empty_like(x) for x in hs]
+    ho = [x.pin_memory() for x in ho]
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    k_e2e = max(3, min(args.steps, 10))
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(k_e2e):
+        for d_, h_ in zip(srcs, hs):
+            d_.copy_(h_, non_blocking=True)
+        call(True)
+        for h_, d_ in zip(ho, dsts):
+            h_.copy_(d_, non_blocking=True)
+    b.record(stream)
+    torch.cuda.synchronize()
+    e_ms = a.elapsed_time(b) / k_e2e
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = batched_cpu_baseline(spec, sides)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "GCells/s", "value": value, "unit": "GCells/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": spec["dtype"], "data": "synthetic (seeded uniform[0,1))",
+            "config": {"workload": name, "grids": spec["ngrids"], "cells": cells,
+                       "sides": "log-uniform [64, 2048], seed 256", "kind": spec["shape"],
+                       "radius": r, "steps_per_call": spec["steps"],
+                       "boundary": spec["boundary"], "parallelism": f"dp{world}",
+                       "l2": f"{2 * cells * es / 2**20:.0f} MiB in+out per pass vs 126 MB L2"},
+            "gpu_launches": launches * args.steps,
+            "per_grid_baseline": {"ms_per_step": ms_pg, "launches_per_step": launches_pg,
+                                  "value": cells * spec["steps"] / (ms_pg / 1e3) / 1e9,
+                                  "speedup_of_persistent": ms_pg / ms},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": load_traffic(name),
+                         "algorithmic_bytes_per_launch": alg_bytes / max(1, launches)},
+            "clocks": clk,
+            "e2e": {"value": cells * spec["steps"] / (e_ms / 1e3) / 1e9, "unit": "GCells/s",
+                    "h2d_bytes_per_step": cells * es, "d2h_bytes_per_step": cells * es,
+                    "steps": k_e2e},
+            "cpu_baseline": cpu,
+        }), flush=True)
+
+
+def batched_cpu_baseline(spec, sides, budget_s=10.0):
+    """Reference Convolution<float> per grid, looped like the reference would
+    run one grid per invocation, on the host cores."""
+    import oracle
+    g = np.random.Generator(np.random.PCG64(3))
+    c = coefficients(spec)
+    r = spec["r"]
+    if spec["shape"] == "star":
+        m = np.zeros((2 * r + 1, 2 * r + 1))
+        m[r, r] = c[0]
+        for k in range(1, r + 1):
+            m[r - k, r], m[r + k, r], m[r, r - k], m[r, r + k] = c[1 + 4 * (k - 1): 5 + 4 * (k - 1)]
+    else:
+        m = np.array(c).reshape(2 * r + 1, 2 * r + 1)
+    m = m.astype(np.float32)
+    t0 = time.perf_counter()
+    cells = 0
+    for h, w_ in sides:
+        x = g.random((int(h), int(w_)), dtype=np.float32)
+        for _ in range(spec["steps"]):
+            x = oracle.ref_convolution(x, m)
+        cells += int(h) * int(w_) * spec["steps"]
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    return {"value": cells / el / 1e9, "unit": "GCells/s", "cores": cores, "kind": "reference",
+            "sample": f"{cells // spec['steps']} cells of the batch x {spec['steps']} steps"}
+
 
 def run_ssam(args, spec, name):
     import torch
@@ -491,6 +643,8 @@ def main(argv=None):
     spec = wl[args.workload]
     if args.impl == "reference":
         run_reference(args, spec, args.workload)
+    elif spec["kind"] == "batched":
+        run_batched(args, spec, args.workload)
     else:
         run_ssam(args, spec, args.workload)
 

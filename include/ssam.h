@@ -203,6 +203,36 @@ SSAM_API int ssam_conv2d(const void* src, void* dst, int64_t width, int64_t pitc
                 int64_t height, int dtype, const double* weight, int fw, int fh,
                 int boundary, void* stream);
 
+/* ------------------------------------------------------- batched 2D grids */
+
+/* One grid of a batch (device pointers, sizes in elements). */
+typedef struct ssam_grid2d {
+  const void* src;
+  void* dst;
+  int64_t width, height, pitch;
+} ssam_grid2d;
+
+typedef enum ssam_batch_mode {
+  /* one cooperative launch steps every grid: warps take tiles from the
+   * flattened tile list of all grids, a grid-wide barrier (bounded wait)
+   * separates the fused-step phases */
+  SSAM_BATCH_PERSISTENT = 0,
+  /* ssam_stencil2d on each grid in turn (one launch chain per grid) */
+  SSAM_BATCH_PER_GRID = 1
+} ssam_batch_mode;
+
+/*
+ * `steps` steps of the same stencil on `ngrids` independent grids of
+ * arbitrary, unequal sizes (same dtype, shape, coefficients, boundary).  The
+ * reference runs one grid per program invocation; this batches them.
+ * Persistent mode is compiled for star/box r = 1, 2 (FP32, FP64, BF16) and
+ * r = 3 (FP32); other stencils return SSAM_ERR_UNSUPPORTED there and run
+ * with SSAM_BATCH_PER_GRID.
+ */
+SSAM_API int ssam_stencil2d_batched(const ssam_grid2d* grids, int ngrids, int dtype,
+                                    int shape, int radius, const double* coeffs, int steps,
+                                    int boundary, int mode, void* stream);
+
 /* -------------------------------------------------------------- autotuner */
 
 /* What the autotuner chose for one stencil and grid size. */

@@ -34,6 +34,15 @@ class SsamError(RuntimeError):
 
 _lib = None
 
+
+class Grid2D(ctypes.Structure):
+    """``ssam_grid2d``: one grid of a batch (device pointers)."""
+    _fields_ = [("src", ctypes.c_void_p), ("dst", ctypes.c_void_p), ("width", ctypes.c_int64),
+                ("height", ctypes.c_int64), ("pitch", ctypes.c_int64)]
+
+
+BATCH_PERSISTENT, BATCH_PER_GRID = 0, 1
+
 _i64 = ctypes.c_int64
 _int = ctypes.c_int
 _vp = ctypes.c_void_p
@@ -59,6 +68,9 @@ def _declare(lib):
     lib.ssam_device_status.restype = _int
     lib.ssam_device_status.argtypes = [_vp]
     lib.ssam_trim_scratch.restype = _int
+    lib.ssam_stencil2d_batched.restype = _int
+    lib.ssam_stencil2d_batched.argtypes = [ctypes.POINTER(Grid2D), _int, _int, _int, _int, _dp,
+                                           _int, _int, _int, _vp]
     lib.ssam_autotune_stencil2d.restype = _int
     lib.ssam_autotune_stencil2d.argtypes = lib.ssam_stencil2d.argtypes + [_vp]
     for name in ("ssam_autotune_save", "ssam_autotune_load"):
@@ -227,6 +239,22 @@ def device_status(stream=None) -> None:
     import torch
     s = stream if stream is not None else torch.cuda.current_stream()
     _check(lib().ssam_device_status(ctypes.c_void_p(s.cuda_stream)))
+
+
+def stencil2d_batched(srcs, coeffs, radius: int, shape: int = STAR, steps: int = 1,
+                      boundary: str = "zero", dsts=None, persistent: bool = True, stream=None):
+    """``ssam_stencil2d_batched`` over a list of 2D CUDA tensors of one dtype."""
+    if dsts is None:
+        dsts = [_grid2d(s_, None) for s_ in srcs]
+    arr = (Grid2D * len(srcs))()
+    for i, (a, b) in enumerate(zip(srcs, dsts)):
+        _grid2d(a, b)
+        arr[i] = Grid2D(a.data_ptr(), b.data_ptr(), a.shape[1], a.shape[0], a.stride(0))
+    _check(lib().ssam_stencil2d_batched(arr, len(srcs), _dtype_code(srcs[0]), shape, radius,
+                                        _doubles(coeffs), steps, BOUNDARY[boundary],
+                                        BATCH_PERSISTENT if persistent else BATCH_PER_GRID,
+                                        _stream_ptr(srcs[0], stream)))
+    return dsts
 
 
 class TuneReport(ctypes.Structure):

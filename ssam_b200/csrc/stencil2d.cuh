@@ -94,6 +94,207 @@ __device__ __forceinline__ void store_row_edge(TS* __restrict__ row, int64_t x0,
     if (x0 + j < W) row[x0 + j] = from_acc<TS>(d[j]);
 }
 
+// One warp's work: the P output rows starting at row y_out0 of the strip
+// whose first output column is x_out0, T fused steps, rows >= y_end not
+// written.  Shared by the grid kernel below and the persistent batched kernel.
+template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int P, int T, int V_>
+__device__ __forceinline__ void stencil2d_warp_tile(
+    const TS* __restrict__ src, TS* __restrict__ dst, int64_t W, int64_t H, int64_t pitch,
+    int64_t x_out0, int64_t y_out0, int64_t y_end, int bnd, int vec_ok,
+    const CoefBlock<typename Traits<TS>::TA, Stencil2DCfg<TS, RL, RR, RT, RB, STAR, P, T, V_>::NC>& cf) {
+  using C = Stencil2DCfg<TS, RL, RR, RT, RB, STAR, P, T, V_>;
+  using TA = typename C::TA;
+  constexpr int V = C::V;
+  constexpr int FW = C::FW;
+  constexpr int ROWS = C::ROWS;
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int64_t x0 = x_out0 + (int64_t)(lane - C::HL) * V;
+  const bool lane_stores = lane >= C::HL && lane < 32 - C::HR;
+  // Does this thread's window touch cells that the boundary rule rewrites?
+  const bool x_edge = bnd == SSAM_BOUNDARY_ZERO
+                          ? (x0 < 0 || x0 + V > W)
+                          : (x0 < RL || x0 + V > W - RR);
+  const int64_t y0 = y_out0 - (int64_t)RT * T;
+  const bool y_edge = bnd == SSAM_BOUNDARY_ZERO
+                          ? (y0 < 0 || y0 + ROWS > H)
+                          : (y0 < RT || y0 + ROWS > H - RB);
+  const bool edge = x_edge || y_edge;
+
+  // ---- register cache: ROWS rows x V columns, 16-byte loads ----------
+  TA d[ROWS][V];
+  const bool row_vec = vec_ok && x0 >= 0 && x0 + V <= W;
+  // Three separate load loops: a branch inside one unrolled loop makes the
+  // compiler keep every path's loads live at once (2-4x the registers).
+  if (row_vec && y0 >= 0 && y0 + ROWS <= H) {
+    // interior: 16-byte loads, one pointer increment per row
+    const TS* p = src + y0 * pitch + x0;
+#pragma unroll
+    for (int k = 0; k < ROWS; ++k) {
+      load_vec<TS, V>(d[k], p);
+      p += pitch;
+    }
+  } else if (row_vec) {
+    // rows beyond the top/bottom edge: zero or clamped row
+#pragma unroll
+    for (int k = 0; k < ROWS; ++k) {
+      int64_t y = y0 + k;
+      if ((y < 0 || y >= H) && bnd == SSAM_BOUNDARY_ZERO) {
+#pragma unroll
+        for (int j = 0; j < V; ++j) d[k][j] = TA(0);
+      } else {
+        y = y < 0 ? 0 : (y >= H ? H - 1 : y);
+        load_vec<TS, V>(d[k], src + y * pitch + x0);
+      }
+    }
+  } else {
+    // columns beyond the left/right edge or unaligned grid: per element
+#pragma unroll 1
+    for (int k = 0; k < ROWS; ++k) {
+      int64_t y = y0 + k;
+      TA v[V];
+      if ((y < 0 || y >= H) && bnd == SSAM_BOUNDARY_ZERO) {
+#pragma unroll
+        for (int j = 0; j < V; ++j) v[j] = TA(0);
+      } else {
+        y = y < 0 ? 0 : (y >= H ? H - 1 : y);
+        load_row_edge<TS, V>(v, src + y * pitch, x0, W, bnd);
+      }
+      // rotate the window so that the row can land in a static slot
+#pragma unroll
+      for (int r = 0; r < ROWS - 1; ++r)
+#pragma unroll
+        for (int j = 0; j < V; ++j) d[r][j] = d[r + 1][j];
+#pragma unroll
+      for (int j = 0; j < V; ++j) d[ROWS - 1][j] = v[j];
+    }
+  }
+
+  // ---- T fused steps; step s rewrites rows [0, ROWS-(RT+RB)(s+1)) ----
+#pragma unroll
+  for (int s = 0; s < T; ++s) {
+    constexpr int FH = RT + RB + 1;
+    const int n_rows = ROWS - (RT + RB) * (s + 1);
+#pragma unroll
+    for (int i = 0; i < ROWS - (RT + RB); ++i) {
+      if (i >= n_rows) break;
+      TA acc[V];
+#pragma unroll
+      for (int j = 0; j < V; ++j) acc[j] = TA(0);
+      // own columns
+#pragma unroll
+      for (int dy = -RT; dy <= RB; ++dy) {
+#pragma unroll
+        for (int dx = -RL; dx <= RR; ++dx) {
+          if (STAR && dy != 0 && dx != 0) continue;
+          const TA w = cf.c[(dy + RT) * FW + (dx + RL)];
+#pragma unroll
+          for (int j = 0; j < V; ++j) {
+            if (j + dx < 0 || j + dx >= V) continue;
+            acc[j] = fma(w, d[i + RT + dy][j + dx], acc[j]);
+          }
+        }
+      }
+      // partial sums travelling right: virtual column V+q, q < RL
+      if constexpr (RL > 0) {
+        TA pr[RL];
+#pragma unroll
+        for (int q = 0; q < RL; ++q) {
+          pr[q] = TA(0);
+#pragma unroll
+          for (int dy = -RT; dy <= RB; ++dy) {
+            if (STAR && dy != 0) continue;
+#pragma unroll
+            for (int j = 0; j < V; ++j) {
+              const int dx = j - V - q;  // source column minus destination
+              if (dx < -RL || dx > -1) continue;
+              pr[q] = fma(cf.c[(dy + RT) * FW + (dx + RL)], d[i + RT + dy][j], pr[q]);
+            }
+          }
+        }
+        constexpr int K = (RL + V - 1) / V;
+#pragma unroll
+        for (int st = K - 1; st >= 0; --st) {
+#pragma unroll
+          for (int q = st * V; q < (st + 1) * V && q < RL; ++q) {
+            const TA v = __shfl_up_sync(FULL, pr[q], 1);
+            if (st == 0) acc[q] += v;
+            else pr[q - V] += v;
+          }
+        }
+      }
+      // partial sums travelling left: virtual column -1-q, q < RR
+      if constexpr (RR > 0) {
+        TA pl[RR];
+#pragma unroll
+        for (int q = 0; q < RR; ++q) {
+          pl[q] = TA(0);
+#pragma unroll
+          for (int dy = -RT; dy <= RB; ++dy) {
+            if (STAR && dy != 0) continue;
+#pragma unroll
+            for (int j = 0; j < V; ++j) {
+              const int dx = j + 1 + q;
+              if (dx < 1 || dx > RR) continue;
+              pl[q] = fma(cf.c[(dy + RT) * FW + (dx + RL)], d[i + RT + dy][j], pl[q]);
+            }
+          }
+        }
+        constexpr int K = (RR + V - 1) / V;
+#pragma unroll
+        for (int st = K - 1; st >= 0; --st) {
+#pragma unroll
+          for (int q = st * V; q < (st + 1) * V && q < RR; ++q) {
+            const TA v = __shfl_down_sync(FULL, pl[q], 1);
+            if (st == 0) acc[V - 1 - q] += v;
+            else pl[q - V] += v;
+          }
+        }
+      }
+      (void)FH;
+      if (T > 1) {
+        // the window row i now holds grid row y0 + RT*(s+1) + i
+        if (edge) {
+          const int64_t y = y0 + (int64_t)RT * (s + 1) + i;
+#pragma unroll
+          for (int j = 0; j < V; ++j)
+            acc[j] = fix_cell<TS, TA>(acc[j], y, x0 + j, W, H, pitch, bnd, RL,
+                                      RR, RT, RB, src);
+        }
+#pragma unroll
+        for (int j = 0; j < V; ++j) d[i][j] = acc[j];
+      } else {
+        // single step: keep the result in place of row i (row i is not
+        // read again), centre value d[i+RT] is still intact for COPY.
+        if (bnd == SSAM_BOUNDARY_COPY && edge) {
+          const int64_t y = y_out0 + i;
+#pragma unroll
+          for (int j = 0; j < V; ++j) {
+            const int64_t x = x0 + j;
+            if ((x < RL) | (x >= W - RR) | (y < RT) | (y >= H - RB))
+              acc[j] = d[i + RT][j];
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < V; ++j) d[i][j] = acc[j];
+      }
+    }
+  }
+
+  // ---- store P rows from the strip's interior lanes ------------------
+  if (lane_stores) {
+    TS* p = dst + y_out0 * pitch;
+#pragma unroll
+    for (int i = 0; i < P; ++i) {
+      if (y_out0 + i < y_end) {
+        if (row_vec) store_vec<TS, V>(p + x0, d[i]);
+        else store_row_edge<TS, V>(p, x0, W, d[i]);
+      }
+      p += pitch;
+    }
+  }
+}
+
 template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int P, int T, int V_>
 __global__ void __launch_bounds__(256)
 stencil2d_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int64_t W,
@@ -102,206 +303,13 @@ stencil2d_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int64_t W,
                  CoefBlock<typename Traits<TS>::TA,
                            Stencil2DCfg<TS, RL, RR, RT, RB, STAR, P, T, V_>::NC> cf) {
   using C = Stencil2DCfg<TS, RL, RR, RT, RB, STAR, P, T, V_>;
-  using TA = typename C::TA;
-  constexpr int V = C::V;
-  constexpr int FW = C::FW;
-  constexpr int ROWS = C::ROWS;
-  constexpr unsigned FULL = 0xffffffffu;
-
-  const int lane = threadIdx.x & 31;
   const int64_t warp_x = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int64_t x_out0 = warp_x * C::OUT_COLS;
   if (x_out0 >= W) return;  // whole warp leaves together
-  const int64_t x0 = x_out0 + (int64_t)(lane - C::HL) * V;
-  const bool lane_stores = lane >= C::HL && lane < 32 - C::HR;
   const int64_t nby = (y_end - y_begin + P - 1) / P;
-
-  // Does this thread's window touch cells that the boundary rule rewrites?
-  const bool x_edge = bnd == SSAM_BOUNDARY_ZERO
-                          ? (x0 < 0 || x0 + V > W)
-                          : (x0 < RL || x0 + V > W - RR);
-
-  for (int64_t by = blockIdx.y; by < nby; by += gridDim.y) {
-    const int64_t y_out0 = y_begin + by * P;
-    const int64_t y0 = y_out0 - (int64_t)RT * T;
-    const bool y_edge = bnd == SSAM_BOUNDARY_ZERO
-                            ? (y0 < 0 || y0 + ROWS > H)
-                            : (y0 < RT || y0 + ROWS > H - RB);
-    const bool edge = x_edge || y_edge;
-
-    // ---- register cache: ROWS rows x V columns, 16-byte loads ----------
-    TA d[ROWS][V];
-    const bool row_vec = vec_ok && x0 >= 0 && x0 + V <= W;
-    // Three separate load loops: a branch inside one unrolled loop makes the
-    // compiler keep every path's loads live at once (2-4x the registers).
-    if (row_vec && y0 >= 0 && y0 + ROWS <= H) {
-      // interior: 16-byte loads, one pointer increment per row
-      const TS* p = src + y0 * pitch + x0;
-#pragma unroll
-      for (int k = 0; k < ROWS; ++k) {
-        load_vec<TS, V>(d[k], p);
-        p += pitch;
-      }
-    } else if (row_vec) {
-      // rows beyond the top/bottom edge: zero or clamped row
-#pragma unroll
-      for (int k = 0; k < ROWS; ++k) {
-        int64_t y = y0 + k;
-        if ((y < 0 || y >= H) && bnd == SSAM_BOUNDARY_ZERO) {
-#pragma unroll
-          for (int j = 0; j < V; ++j) d[k][j] = TA(0);
-        } else {
-          y = y < 0 ? 0 : (y >= H ? H - 1 : y);
-          load_vec<TS, V>(d[k], src + y * pitch + x0);
-        }
-      }
-    } else {
-      // columns beyond the left/right edge or unaligned grid: per element
-#pragma unroll 1
-      for (int k = 0; k < ROWS; ++k) {
-        int64_t y = y0 + k;
-        TA v[V];
-        if ((y < 0 || y >= H) && bnd == SSAM_BOUNDARY_ZERO) {
-#pragma unroll
-          for (int j = 0; j < V; ++j) v[j] = TA(0);
-        } else {
-          y = y < 0 ? 0 : (y >= H ? H - 1 : y);
-          load_row_edge<TS, V>(v, src + y * pitch, x0, W, bnd);
-        }
-        // rotate the window so that the row can land in a static slot
-#pragma unroll
-        for (int r = 0; r < ROWS - 1; ++r)
-#pragma unroll
-          for (int j = 0; j < V; ++j) d[r][j] = d[r + 1][j];
-#pragma unroll
-        for (int j = 0; j < V; ++j) d[ROWS - 1][j] = v[j];
-      }
-    }
-
-    // ---- T fused steps; step s rewrites rows [0, ROWS-(RT+RB)(s+1)) ----
-#pragma unroll
-    for (int s = 0; s < T; ++s) {
-      constexpr int FH = RT + RB + 1;
-      const int n_rows = ROWS - (RT + RB) * (s + 1);
-#pragma unroll
-      for (int i = 0; i < ROWS - (RT + RB); ++i) {
-        if (i >= n_rows) break;
-        TA acc[V];
-#pragma unroll
-        for (int j = 0; j < V; ++j) acc[j] = TA(0);
-        // own columns
-#pragma unroll
-        for (int dy = -RT; dy <= RB; ++dy) {
-#pragma unroll
-          for (int dx = -RL; dx <= RR; ++dx) {
-            if (STAR && dy != 0 && dx != 0) continue;
-            const TA w = cf.c[(dy + RT) * FW + (dx + RL)];
-#pragma unroll
-            for (int j = 0; j < V; ++j) {
-              if (j + dx < 0 || j + dx >= V) continue;
-              acc[j] = fma(w, d[i + RT + dy][j + dx], acc[j]);
-            }
-          }
-        }
-        // partial sums travelling right: virtual column V+q, q < RL
-        if constexpr (RL > 0) {
-          TA pr[RL];
-#pragma unroll
-          for (int q = 0; q < RL; ++q) {
-            pr[q] = TA(0);
-#pragma unroll
-            for (int dy = -RT; dy <= RB; ++dy) {
-              if (STAR && dy != 0) continue;
-#pragma unroll
-              for (int j = 0; j < V; ++j) {
-                const int dx = j - V - q;  // source column minus destination
-                if (dx < -RL || dx > -1) continue;
-                pr[q] = fma(cf.c[(dy + RT) * FW + (dx + RL)], d[i + RT + dy][j], pr[q]);
-              }
-            }
-          }
-          constexpr int K = (RL + V - 1) / V;
-#pragma unroll
-          for (int st = K - 1; st >= 0; --st) {
-#pragma unroll
-            for (int q = st * V; q < (st + 1) * V && q < RL; ++q) {
-              const TA v = __shfl_up_sync(FULL, pr[q], 1);
-              if (st == 0) acc[q] += v;
-              else pr[q - V] += v;
-            }
-          }
-        }
-        // partial sums travelling left: virtual column -1-q, q < RR
-        if constexpr (RR > 0) {
-          TA pl[RR];
-#pragma unroll
-          for (int q = 0; q < RR; ++q) {
-            pl[q] = TA(0);
-#pragma unroll
-            for (int dy = -RT; dy <= RB; ++dy) {
-              if (STAR && dy != 0) continue;
-#pragma unroll
-              for (int j = 0; j < V; ++j) {
-                const int dx = j + 1 + q;
-                if (dx < 1 || dx > RR) continue;
-                pl[q] = fma(cf.c[(dy + RT) * FW + (dx + RL)], d[i + RT + dy][j], pl[q]);
-              }
-            }
-          }
-          constexpr int K = (RR + V - 1) / V;
-#pragma unroll
-          for (int st = K - 1; st >= 0; --st) {
-#pragma unroll
-            for (int q = st * V; q < (st + 1) * V && q < RR; ++q) {
-              const TA v = __shfl_down_sync(FULL, pl[q], 1);
-              if (st == 0) acc[V - 1 - q] += v;
-              else pl[q - V] += v;
-            }
-          }
-        }
-        (void)FH;
-        if (T > 1) {
-          // the window row i now holds grid row y0 + RT*(s+1) + i
-          if (edge) {
-            const int64_t y = y0 + (int64_t)RT * (s + 1) + i;
-#pragma unroll
-            for (int j = 0; j < V; ++j)
-              acc[j] = fix_cell<TS, TA>(acc[j], y, x0 + j, W, H, pitch, bnd, RL,
-                                        RR, RT, RB, src);
-          }
-#pragma unroll
-          for (int j = 0; j < V; ++j) d[i][j] = acc[j];
-        } else {
-          // single step: keep the result in place of row i (row i is not
-          // read again), centre value d[i+RT] is still intact for COPY.
-          if (bnd == SSAM_BOUNDARY_COPY && edge) {
-            const int64_t y = y_out0 + i;
-#pragma unroll
-            for (int j = 0; j < V; ++j) {
-              const int64_t x = x0 + j;
-              if ((x < RL) | (x >= W - RR) | (y < RT) | (y >= H - RB))
-                acc[j] = d[i + RT][j];
-            }
-          }
-#pragma unroll
-          for (int j = 0; j < V; ++j) d[i][j] = acc[j];
-        }
-      }
-    }
-
-    // ---- store P rows from the strip's interior lanes ------------------
-    if (lane_stores) {
-      TS* p = dst + y_out0 * pitch;
-#pragma unroll
-      for (int i = 0; i < P; ++i) {
-        if (y_out0 + i < y_end) {
-          if (row_vec) store_vec<TS, V>(p + x0, d[i]);
-          else store_row_edge<TS, V>(p, x0, W, d[i]);
-        }
-        p += pitch;
-      }
-    }
-  }
+  for (int64_t by = blockIdx.y; by < nby; by += gridDim.y)
+    stencil2d_warp_tile<TS, RL, RR, RT, RB, STAR, P, T, V_>(
+        src, dst, W, H, pitch, x_out0, y_begin + by * P, y_end, bnd, vec_ok, cf);
 }
 
 template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int P, int T, int V_>

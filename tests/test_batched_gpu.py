@@ -1,0 +1,77 @@
+"""Many uneven grids in one persistent launch (ssam_stencil2d_batched) give
+the oracle's result on every grid, and the same bits as stepping each grid
+with its own launches."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+import ssam_b200 as S
+from ssam_cases import assert_rel_close, magnitude2d, normalised, rng, star_matrix
+
+pytestmark = pytest.mark.gpu
+
+
+def _grids(n, lo, hi, seed, dt=np.float32):
+    g = rng(seed)
+    sides = np.exp(g.uniform(np.log(lo), np.log(hi), size=(n, 2))).astype(int)
+    return [g.uniform(0, 1, size=(int(h), int(w))).astype(dt) for h, w in sides]
+
+
+@pytest.mark.parametrize("kind,r", [("star", 1), ("box", 2), ("box", 1), ("star", 2),
+                                    ("box", 3)])
+@pytest.mark.parametrize("steps", [1, 3, 7, 50])
+@pytest.mark.parametrize("bnd", ["zero", "copy"])
+def test_batched_vs_oracle_and_per_grid(cuda, kind, r, steps, bnd):
+    hosts = _grids(12, 9, 300, hash((kind, r, steps)) % 2**31)
+    if kind == "star":
+        c = normalised((4 * r + 1,), r)
+        m = star_matrix(c, r)
+        shape = S.STAR
+    else:
+        m = normalised((2 * r + 1, 2 * r + 1), r)
+        c = m.ravel()
+        shape = S.BOX
+    srcs = [torch.from_numpy(h).to(cuda) for h in hosts]
+    got = S.stencil2d_batched(srcs, c, r, shape, steps, bnd, persistent=True)
+    ref = S.stencil2d_batched(srcs, c, r, shape, steps, bnd, persistent=False)
+    S.device_status()
+    for h, a, b in zip(hosts, got, ref):
+        a = a.cpu().numpy()
+        want = oracle.conv2d(h, m.astype(np.float32), bnd, steps=steps)
+        assert_rel_close(a, want, magnitude2d(h, m, bnd, steps), 1e-5 * steps, f"{h.shape}")
+        np.testing.assert_array_equal(a, b.cpu().numpy())
+
+
+@pytest.mark.parametrize("tdt", [torch.float64, torch.bfloat16])
+def test_batched_other_dtypes(cuda, tdt):
+    hosts = _grids(6, 20, 200, 5)
+    c = normalised((5,), 1)
+    m = star_matrix(c, 1)
+    srcs = [torch.from_numpy(h).to(tdt).to(cuda) for h in hosts]
+    got = S.stencil2d_batched(srcs, c, 1, S.STAR, 9, "copy")
+    for s_, a in zip(srcs, got):
+        x = s_.double().cpu().numpy()
+        want = oracle.conv2d(x, m, "copy", steps=9)
+        rel = 1e-12 * 9 if tdt == torch.float64 else 2.0**-8 * 9
+        scale = np.maximum(np.abs(want), magnitude2d(x, m, "copy", 9))
+        assert_rel_close(a.double().cpu().numpy(), want, scale, rel, str(tdt))
+
+
+def test_batched_256_uneven_grids_config4(cuda):
+    """The benchmark batch: 256 grids, sides log-uniform in [64, 2048], 5-pt,
+    50 steps; persistent == per-grid launches bit for bit, and grid 0 against
+    the oracle."""
+    g = rng(256)
+    sides = np.exp(g.uniform(np.log(64), np.log(2048), size=(256, 2))).astype(int)
+    srcs = [torch.rand(int(h), int(w), device=cuda) for h, w in sides]
+    c = [0.2] * 5
+    got = S.stencil2d_batched(srcs, c, 1, S.STAR, 50, "copy", persistent=True)
+    ref = S.stencil2d_batched(srcs, c, 1, S.STAR, 50, "copy", persistent=False)
+    S.device_status()
+    for a, b in zip(got, ref):
+        assert torch.equal(a, b)
+    h0 = srcs[0].cpu().numpy()
+    m = star_matrix(c, 1)
+    want = oracle.conv2d(h0, m.astype(np.float32), "copy", steps=50)
+    assert_rel_close(got[0].cpu().numpy(), want, magnitude2d(h0, m, "copy", 50), 5e-4, "g0")
