@@ -296,6 +296,53 @@ SSAM_API int ssam_stencil3d_host(const void* h_src, void* h_dst, int64_t nx, int
                                  const double* coeffs, int steps, int boundary,
                                  void* stream);
 
+/* ---------------------------------------------------------------- Poisson */
+
+/*
+ * -lap(u) = f on the unit cube with u = 0 on the boundary, discretised with the
+ * 7-point operator on n^3 interior points (h = 1/(n+1)); `nbatch` independent
+ * right-hand sides stored one after the other (index ((b*n + z)*n + y)*n + x).
+ * No counterpart in the reference: its "poisson" program applies a 19-point
+ * operator (tmpPoisson.cu); the solver follows its 7-point stencil structure
+ * (v2::j3d7pt_gold, tmp3d7pt-v2.cu:281-297).
+ */
+typedef struct ssam_poisson_options {
+  double tol;                /* stop when ||f - A u||_2 / ||f||_2 <= tol for every rhs */
+  int sweep_dtype;           /* SSAM_F32 or SSAM_BF16: storage of the Jacobi sweeps */
+  int sweeps_per_correction; /* Jacobi sweeps between two FP64 residuals */
+  int max_sweeps;            /* give up (converged = 0) after this many sweeps */
+} ssam_poisson_options;
+
+typedef struct ssam_poisson_stats {
+  int converged;               /* every rhs reached tol */
+  int sweeps;                  /* Jacobi sweeps run */
+  int corrections;             /* FP64 defect-correction steps */
+  double initial_rel_residual; /* max over the batch, for the initial guess */
+  double rel_residual;         /* max over the batch, final (FP64) */
+} ssam_poisson_stats;
+
+/*
+ * Defect correction: r = f - A u in FP64; e ~= A^-1 r by `sweeps_per_correction`
+ * Jacobi sweeps from 0 in sweep_dtype storage with FP32 arithmetic; u += e in
+ * FP64; until tol.  `u` (device, FP64) holds the initial guess on entry (zeros
+ * for the plain method, a learned warm start otherwise) and the solution on
+ * return.  Synchronous: it reads the residual norms on the host.
+ */
+SSAM_API int ssam_poisson_solve(const double* f, double* u, int n, int nbatch,
+                                const ssam_poisson_options* opt, ssam_poisson_stats* stats,
+                                void* stream);
+
+/* ||f - A u||_2 / ||f||_2 per right-hand side, in FP64 (`rel` is host, nbatch). */
+SSAM_API int ssam_poisson_residual(const double* f, const double* u, int n, int nbatch,
+                                   double* rel, void* stream);
+
+/*
+ * `sweeps` plain Jacobi sweeps u <- (sum of the 6 neighbours + h^2 rhs) / 6 in
+ * `dtype` storage (F32, BF16 or F64), from u_in into u_out (u_in != u_out).
+ */
+SSAM_API int ssam_poisson_jacobi(const void* rhs, const void* u_in, void* u_out, int n,
+                                 int nbatch, int dtype, int sweeps, void* stream);
+
 /*
  * Synchronises `stream` and reports whether a bounded device-side wait of
  * any kernel on the current device gave up since the last call

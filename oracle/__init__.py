@@ -189,3 +189,31 @@ def rms_max_error(out: np.ndarray, ref_: np.ndarray, lo: int, hi_off: int):
         _i64(lo), _i64(ny - hi_off), _i64(lo), _i64(nx - hi_off),
         ctypes.byref(rms), ctypes.byref(mx))
     return rms.value, mx.value
+
+
+# ---------------------------------------------------------------- Poisson --
+
+def jacobi7(rhs: np.ndarray, u: np.ndarray, sweeps: int) -> np.ndarray:
+    """FP64 Jacobi sweeps of -lap(u) = rhs, Dirichlet 0, shape (nb, n, n, n)."""
+    rhs = np.ascontiguousarray(rhs, np.float64)
+    u = np.ascontiguousarray(u, np.float64)
+    nb, n = rhs.shape[0], rhs.shape[1]
+    out = np.empty_like(u)
+    work = np.empty_like(u)
+    if sweeps == 0:
+        return u.copy()
+    lib().ssam_oracle_jacobi7_f64(_ptr(rhs), _ptr(u), _ptr(out), _i64(n), _i64(nb),
+                                  ctypes.c_int(sweeps), _ptr(work))
+    return out
+
+
+def residual7(f: np.ndarray, u: np.ndarray):
+    """(r, rel) with r = f - A u and rel = ||r|| / ||f|| per right-hand side."""
+    f = np.ascontiguousarray(f, np.float64)
+    u = np.ascontiguousarray(u, np.float64)
+    nb, n = f.shape[0], f.shape[1]
+    r = np.empty_like(f)
+    norms = np.zeros(2 * nb)
+    lib().ssam_oracle_residual7_f64(_ptr(f), _ptr(u), _ptr(r), _i64(n), _i64(nb), _ptr(norms))
+    return r, np.sqrt(norms[0::2] / norms[1::2])
+

@@ -214,3 +214,77 @@ void ssam_oracle_check_error3d_f64(const double* out, const double* ref,
   *rms = sqrt(err / (double)((z_ub - z_lb) * (y_ub - y_lb) * (x_ub - x_lb)));
   *max_err = mx;
 }
+
+/* ------------------------------------------------------------- Poisson --- */
+
+/*
+ * No reference code exists for the Poisson solver; these restate the
+ * mathematics in FP64 with the loop structure of v2::j3d7pt_gold
+ * (ssai-3dstencil/tmp3d7pt-v2.cu:281-297): z outer (OpenMP), y, x inner.
+ * Grids: `nb` stacked n^3 interior grids, u = 0 outside (Dirichlet),
+ * h = 1/(n+1).
+ *
+ * One Jacobi sweep: out = (sum of the 6 neighbours of in + h^2 rhs) / 6,
+ * neighbours summed in the order z-1, y-1, x-1, x+1, y+1, z+1.
+ */
+void ssam_oracle_jacobi7_f64(const double* rhs, const double* in, double* out, int64_t n,
+                             int64_t nb, int sweeps, double* work) {
+  const double h2 = 1.0 / (double)((n + 1) * (n + 1));
+  const int64_t nn = n * n, n3 = n * n * n;
+  const double* src = in;
+  for (int s = 0; s < sweeps; s++) {
+    double* dst = ((sweeps - 1 - s) % 2 == 0) ? out : work;
+    for (int64_t b = 0; b < nb; b++) {
+      const double* u = src + b * n3;
+      const double* f = rhs + b * n3;
+      double* o = dst + b * n3;
+      _Pragma("omp parallel for schedule(static)")
+      for (int64_t k = 0; k < n; k++)
+        for (int64_t j = 0; j < n; j++)
+          for (int64_t i = 0; i < n; i++) {
+            const int64_t c = k * nn + j * n + i;
+            double sum = 0.0;
+            if (k > 0) sum += u[c - nn];
+            if (j > 0) sum += u[c - n];
+            if (i > 0) sum += u[c - 1];
+            if (i < n - 1) sum += u[c + 1];
+            if (j < n - 1) sum += u[c + n];
+            if (k < n - 1) sum += u[c + nn];
+            o[c] = (sum + h2 * f[c]) / 6.0;
+          }
+    }
+    src = dst;
+  }
+}
+
+/* r = f - A u with A u = (6 u - sum of neighbours) / h^2; per-grid
+ * sum r^2 and sum f^2 into norms2[2*b], norms2[2*b+1]. */
+void ssam_oracle_residual7_f64(const double* f, const double* u, double* r, int64_t n,
+                               int64_t nb, double* norms2) {
+  const double inv_h2 = (double)((n + 1) * (n + 1));
+  const int64_t nn = n * n, n3 = n * n * n;
+  for (int64_t b = 0; b < nb; b++) {
+    const double* ub = u + b * n3;
+    const double* fb = f + b * n3;
+    double rr = 0.0, ff = 0.0;
+    _Pragma("omp parallel for schedule(static) reduction(+:rr,ff)")
+    for (int64_t k = 0; k < n; k++)
+      for (int64_t j = 0; j < n; j++)
+        for (int64_t i = 0; i < n; i++) {
+          const int64_t c = k * nn + j * n + i;
+          double sum = 0.0;
+          if (k > 0) sum += ub[c - nn];
+          if (j > 0) sum += ub[c - n];
+          if (i > 0) sum += ub[c - 1];
+          if (i < n - 1) sum += ub[c + 1];
+          if (j < n - 1) sum += ub[c + n];
+          if (k < n - 1) sum += ub[c + nn];
+          const double rc = fb[c] - (6.0 * ub[c] - sum) * inv_h2;
+          if (r) r[b * n3 + c] = rc;
+          rr += rc * rc;
+          ff += fb[c] * fb[c];
+        }
+    norms2[2 * b] = rr;
+    norms2[2 * b + 1] = ff;
+  }
+}

@@ -43,6 +43,19 @@ class Grid2D(ctypes.Structure):
 
 BATCH_PERSISTENT, BATCH_PER_GRID = 0, 1
 
+
+class PoissonOptions(ctypes.Structure):
+    """``ssam_poisson_options``."""
+    _fields_ = [("tol", ctypes.c_double), ("sweep_dtype", ctypes.c_int),
+                ("sweeps_per_correction", ctypes.c_int), ("max_sweeps", ctypes.c_int)]
+
+
+class PoissonStats(ctypes.Structure):
+    """``ssam_poisson_stats``."""
+    _fields_ = [("converged", ctypes.c_int), ("sweeps", ctypes.c_int),
+                ("corrections", ctypes.c_int), ("initial_rel_residual", ctypes.c_double),
+                ("rel_residual", ctypes.c_double)]
+
 _i64 = ctypes.c_int64
 _int = ctypes.c_int
 _vp = ctypes.c_void_p
@@ -71,6 +84,13 @@ def _declare(lib):
     lib.ssam_stencil2d_batched.restype = _int
     lib.ssam_stencil2d_batched.argtypes = [ctypes.POINTER(Grid2D), _int, _int, _int, _int, _dp,
                                            _int, _int, _int, _vp]
+    lib.ssam_poisson_solve.restype = _int
+    lib.ssam_poisson_solve.argtypes = [_vp, _vp, _int, _int, ctypes.POINTER(PoissonOptions),
+                                       ctypes.POINTER(PoissonStats), _vp]
+    lib.ssam_poisson_residual.restype = _int
+    lib.ssam_poisson_residual.argtypes = [_vp, _vp, _int, _int, _dp, _vp]
+    lib.ssam_poisson_jacobi.restype = _int
+    lib.ssam_poisson_jacobi.argtypes = [_vp, _vp, _vp, _int, _int, _int, _int, _vp]
     lib.ssam_autotune_stencil2d.restype = _int
     lib.ssam_autotune_stencil2d.argtypes = lib.ssam_stencil2d.argtypes + [_vp]
     for name in ("ssam_autotune_save", "ssam_autotune_load"):
@@ -255,6 +275,49 @@ def stencil2d_batched(srcs, coeffs, radius: int, shape: int = STAR, steps: int =
                                         BATCH_PERSISTENT if persistent else BATCH_PER_GRID,
                                         _stream_ptr(srcs[0], stream)))
     return dsts
+
+
+def _poisson_grid(t):
+    if not t.is_cuda or t.dim() != 4 or t.shape[1] != t.shape[2] or t.shape[2] != t.shape[3] \
+            or not t.is_contiguous():
+        raise ValueError("Poisson grids are contiguous CUDA tensors of shape (nbatch, n, n, n)")
+    return t.shape[0], t.shape[1]
+
+
+def poisson_solve(f, u, tol: float = 1e-5, sweep_dtype=None, sweeps_per_correction: int = 1000,
+                  max_sweeps: int = 200000, stream=None) -> dict:
+    """``ssam_poisson_solve``: f, u are float64 (nbatch, n, n, n); u holds the
+    initial guess and receives the solution."""
+    import torch
+    nb, n = _poisson_grid(f)
+    if u.shape != f.shape or f.dtype != torch.float64 or u.dtype != torch.float64:
+        raise ValueError("f and u must be float64 tensors of the same shape")
+    dt = F32 if sweep_dtype in (None, "f32", torch.float32) else BF16
+    opt = PoissonOptions(tol, dt, sweeps_per_correction, max_sweeps)
+    st = PoissonStats()
+    _check(lib().ssam_poisson_solve(f.data_ptr(), u.data_ptr(), n, nb, ctypes.byref(opt),
+                                    ctypes.byref(st), _stream_ptr(f, stream)))
+    return {k: getattr(st, k) for k, _ in st._fields_}
+
+
+def poisson_residual(f, u, stream=None) -> list:
+    """FP64 ||f - A u|| / ||f|| per right-hand side."""
+    nb, n = _poisson_grid(f)
+    rel = (ctypes.c_double * nb)()
+    _check(lib().ssam_poisson_residual(f.data_ptr(), u.data_ptr(), n, nb, rel,
+                                       _stream_ptr(f, stream)))
+    return list(rel)
+
+
+def poisson_jacobi(rhs, u_in, sweeps: int, u_out=None, stream=None):
+    """``sweeps`` Jacobi sweeps in the storage type of the tensors."""
+    import torch
+    nb, n = _poisson_grid(rhs)
+    if u_out is None:
+        u_out = torch.empty_like(u_in)
+    _check(lib().ssam_poisson_jacobi(rhs.data_ptr(), u_in.data_ptr(), u_out.data_ptr(), n, nb,
+                                     _dtype_code(rhs), sweeps, _stream_ptr(rhs, stream)))
+    return u_out
 
 
 class TuneReport(ctypes.Structure):

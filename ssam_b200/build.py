@@ -29,7 +29,8 @@ NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
            "-Wno-deprecated-gpu-targets"]
 
 # Hand-written (non-generated) translation units.
-SOURCES = ["api.cu", "autotune.cu", "stencil3d.cu", "noalloc.cu", "batched.cu"]
+SOURCES = ["api.cu", "autotune.cu", "stencil3d.cu", "noalloc.cu", "batched.cu",
+           "poisson.cu"]
 
 DTYPES = {"f32": "float", "f64": "double", "bf16": "__nv_bfloat16", "f16": "__half"}
 

@@ -176,14 +176,23 @@ int pick_2d(int dtype, int rl, int rr, int rt, int rb, int star, int t,
 
 // A kernel fusing `t` steps is compiled for this stencil (any P).
 bool have_depth_2d(int dtype, int rl, int rr, int rt, int rb, int star, int t) {
-  struct Acc { int t; bool found; } acc{t, false};
-  list_2d(dtype, rl, rr, rt, rb, star,
-          [](const Key2D& k, const Kernel2DInfo&, void* u) {
-            Acc* a = (Acc*)u;
-            if (k.t == a->t) a->found = true;
-          },
-          &acc);
-  return acc.found;
+  // bit t of the mask: some kernel fuses t steps (computed once per stencil;
+  // the registry is complete before the first call)
+  static std::mutex mu;
+  static std::map<std::vector<int>, unsigned> masks;
+  const std::vector<int> key{dtype, rl, rr, rt, rb, star};
+  std::lock_guard<std::mutex> g(mu);
+  auto it = masks.find(key);
+  if (it == masks.end()) {
+    unsigned m = 0;
+    list_2d(dtype, rl, rr, rt, rb, star,
+            [](const Key2D& k, const Kernel2DInfo&, void* u) {
+              if (k.t < 32) *(unsigned*)u |= 1u << k.t;
+            },
+            &m);
+    it = masks.emplace(key, m).first;
+  }
+  return t >= 0 && t < 32 && (it->second >> t) & 1u;
 }
 
 // Runs `steps` steps as a chain of launches of <= the tuned temporal depth,

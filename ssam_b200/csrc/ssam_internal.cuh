@@ -29,6 +29,8 @@ int run_3d(const void* src, void* dst, int64_t nx, int64_t ny, int64_t nz, int d
            int shape, int r, const double* coef, int steps, int boundary, int use_graph,
            cudaStream_t stream);
 int device_error_word(int** out);
+int sweep_3d(const void* in, void* out, int64_t n, int nb, int dtype, const double* cube,
+             const void* rhs, double rhs_scale, cudaStream_t s);
 
 // Stream-ordered device scratch from the library's per-device pool.
 int scratch_alloc(void** p, size_t bytes, cudaStream_t s);

@@ -123,18 +123,30 @@ __device__ __forceinline__ void stencil2d_warp_tile(
 
   // ---- register cache: ROWS rows x V columns, 16-byte loads ----------
   TA d[ROWS][V];
-  const bool row_vec = vec_ok && x0 >= 0 && x0 + V <= W;
-  // Three separate load loops: a branch inside one unrolled loop makes the
-  // compiler keep every path's loads live at once (2-4x the registers).
-  if (row_vec && y0 >= 0 && y0 + ROWS <= H) {
-    // interior: 16-byte loads, one pointer increment per row
+  // Columns of this thread inside the grid?  Then rows are read whole: with
+  // 16-byte loads when the grid is 16-byte aligned (vec_ok), else with one
+  // load per element.  Separate loops per case: a branch inside one unrolled
+  // loop makes the compiler keep every path's loads live (2-4x registers).
+  const bool cols_in = x0 >= 0 && x0 + V <= W;
+  const bool row_vec = vec_ok && cols_in;
+  const bool rows_in = y0 >= 0 && y0 + ROWS <= H;
+  if (cols_in && rows_in) {
     const TS* p = src + y0 * pitch + x0;
+    if (vec_ok) {
 #pragma unroll
-    for (int k = 0; k < ROWS; ++k) {
-      load_vec<TS, V>(d[k], p);
-      p += pitch;
+      for (int k = 0; k < ROWS; ++k) {
+        load_vec<TS, V>(d[k], p);
+        p += pitch;
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < ROWS; ++k) {
+#pragma unroll
+        for (int j = 0; j < V; ++j) d[k][j] = to_acc(__ldg(p + j));
+        p += pitch;
+      }
     }
-  } else if (row_vec) {
+  } else if (cols_in) {
     // rows beyond the top/bottom edge: zero or clamped row
 #pragma unroll
     for (int k = 0; k < ROWS; ++k) {
@@ -144,11 +156,17 @@ __device__ __forceinline__ void stencil2d_warp_tile(
         for (int j = 0; j < V; ++j) d[k][j] = TA(0);
       } else {
         y = y < 0 ? 0 : (y >= H ? H - 1 : y);
-        load_vec<TS, V>(d[k], src + y * pitch + x0);
+        const TS* p = src + y * pitch + x0;
+        if (vec_ok) {
+          load_vec<TS, V>(d[k], p);
+        } else {
+#pragma unroll
+          for (int j = 0; j < V; ++j) d[k][j] = to_acc(__ldg(p + j));
+        }
       }
     }
   } else {
-    // columns beyond the left/right edge or unaligned grid: per element
+    // columns beyond the left/right edge (edge lanes only): per element
 #pragma unroll 1
     for (int k = 0; k < ROWS; ++k) {
       int64_t y = y0 + k;
@@ -287,8 +305,14 @@ __device__ __forceinline__ void stencil2d_warp_tile(
 #pragma unroll
     for (int i = 0; i < P; ++i) {
       if (y_out0 + i < y_end) {
-        if (row_vec) store_vec<TS, V>(p + x0, d[i]);
-        else store_row_edge<TS, V>(p, x0, W, d[i]);
+        if (row_vec) {
+          store_vec<TS, V>(p + x0, d[i]);
+        } else if (cols_in) {
+#pragma unroll
+          for (int j = 0; j < V; ++j) p[x0 + j] = from_acc<TS>(d[i][j]);
+        } else {
+          store_row_edge<TS, V>(p, x0, W, d[i]);
+        }
       }
       p += pitch;
     }

@@ -58,6 +58,9 @@ struct Launch3D {
   const void* src;
   void* dst;
   int64_t nx, ny, nz;
+  int nb;              // grids stacked along a 4th axis (1 = plain 3D grid)
+  const void* rhs;     // NULL, or out += rhs_scale * rhs
+  double rhs_scale;
   const double* coef;  // (2R+1)^3, [dz][dy][dx]
   int boundary;
   cudaStream_t stream;
@@ -95,6 +98,9 @@ static int launch_3d(const Launch3D& a) {
   w.nx = a.nx;
   w.ny = a.ny;
   w.nz = a.nz;
+  w.nb = a.nb;
+  w.rhs = a.rhs;
+  w.rhs_scale = a.rhs_scale;
   w.ntx = (int)((a.nx + C::TX - 1) / C::TX);
   w.nty = (int)((a.ny + C::TY - 1) / C::TY);
   // z chunk: minimise (rounds of items) x (chunk + 2R prologue planes)
@@ -103,7 +109,7 @@ static int launch_3d(const Launch3D& a) {
   int64_t best = -1;
   for (int zc : {8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512}) {
     if (zc > 2 * a.nz && zc > 8) break;
-    const int64_t items = ntiles * ((a.nz + zc - 1) / zc);
+    const int64_t items = ntiles * ((a.nz + zc - 1) / zc) * a.nb;
     const int64_t rounds = (items + grid_max - 1) / grid_max;
     const int64_t cost = rounds * (std::min<int64_t>(zc, a.nz) + 2 * R);
     if (best < 0 || cost < best) {
@@ -124,11 +130,13 @@ static int launch_3d(const Launch3D& a) {
   w.use_tma = ((uintptr_t)a.src % 16 == 0) && ((a.nx * (int64_t)es) % 16 == 0) &&
               a.nx <= (int64_t(1) << 32) && encode_fn() != nullptr;
   if (w.use_tma) {
-    cuuint64_t dims[3] = {(cuuint64_t)a.nx, (cuuint64_t)a.ny, (cuuint64_t)a.nz};
-    cuuint64_t strides[2] = {(cuuint64_t)(a.nx * es), (cuuint64_t)(a.nx * a.ny * es)};
-    cuuint32_t box[3] = {(cuuint32_t)C::XW, (cuuint32_t)C::YW, 1};
-    cuuint32_t estr[3] = {1, 1, 1};
-    CUresult r = encode_fn()(&map, tma_dtype<TS>(), 3, const_cast<void*>(a.src), dims,
+    cuuint64_t dims[4] = {(cuuint64_t)a.nx, (cuuint64_t)a.ny, (cuuint64_t)a.nz,
+                          (cuuint64_t)a.nb};
+    cuuint64_t strides[3] = {(cuuint64_t)(a.nx * es), (cuuint64_t)(a.nx * a.ny * es),
+                             (cuuint64_t)(a.nx * a.ny * a.nz * es)};
+    cuuint32_t box[4] = {(cuuint32_t)C::XW, (cuuint32_t)C::YW, 1, 1};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = encode_fn()(&map, tma_dtype<TS>(), 4, const_cast<void*>(a.src), dims,
                              strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -229,7 +237,7 @@ static int enqueue_chain_3d(LaunchFn3D fn, const GraphKey& k, void* scratch,
   const void* in = k.src;
   for (int i = 0; i < k.steps; ++i) {
     void* out = ((k.steps - 1 - i) % 2 == 0) ? k.dst : scratch;
-    Launch3D a{in, out, k.nx, k.ny, k.nz, k.coef.data(), k.boundary, s, false};
+    Launch3D a{in, out, k.nx, k.ny, k.nz, 1, nullptr, 0.0, k.coef.data(), k.boundary, s, false};
     int st = fn(a);
     if (st != SSAM_OK) return st;
     in = out;
@@ -286,7 +294,8 @@ int run_3d(const void* src, void* dst, int64_t nx, int64_t ny, int64_t nz, int d
     int st = scratch_alloc(&e.scratch, bytes, stream);
     if (st != SSAM_OK) return st;
     SSAM_CUDA_TRY(cudaStreamSynchronize(stream));
-    Launch3D prep{k.src, k.dst, k.nx, k.ny, k.nz, k.coef.data(), k.boundary, stream, true};
+    Launch3D prep{k.src, k.dst, k.nx, k.ny, k.nz, 1, nullptr, 0.0, k.coef.data(), k.boundary,
+                  stream, true};
     st = fn(prep);
     if (st != SSAM_OK) return st;
     cudaStream_t cs = nullptr;
@@ -323,6 +332,21 @@ int drop_graphs_3d() {
   }
   g_graphs.clear();
   return SSAM_OK;
+}
+
+}  // namespace ssam
+
+namespace ssam {
+
+// One launch of the 3D star kernel (r = 1) over `nb` stacked n^3 grids with an
+// optional right-hand side: out = stencil(in) + rhs_scale * rhs, zero
+// (Dirichlet) boundary.  Used by the Poisson Jacobi sweeps.
+int sweep_3d(const void* in, void* out, int64_t n, int nb, int dtype, const double* cube,
+             const void* rhs, double rhs_scale, cudaStream_t s) {
+  LaunchFn3D fn = find_3d(dtype, SH3_STAR, 1);
+  if (!fn) return fail(SSAM_ERR_UNSUPPORTED, "no 3D 7-point kernel for this dtype");
+  Launch3D a{in, out, n, n, n, nb, rhs, rhs_scale, cube, SSAM_BOUNDARY_ZERO, s, false};
+  return fn(a);
 }
 
 }  // namespace ssam

@@ -85,9 +85,12 @@ struct Stencil3DCfg {
 
 struct Work3D {
   int64_t nx, ny, nz;
+  int nb;                // independent grids stacked along a 4th axis
   int ntx, nty;          // column tiles
   int zc;                // planes per work item (z chunk)
-  int64_t items;         // ntx*nty*ceil(nz/zc) (chunk, tile) work items
+  int64_t items;         // nb*ntx*nty*ceil(nz/zc) (grid, chunk, tile) work items
+  const void* rhs;       // optional: out += rhs_scale * rhs (same layout), else NULL
+  double rhs_scale;
   int boundary;
   int use_tma;
   unsigned long long wait_ns;
@@ -139,12 +142,15 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned par, unsigned lo
     if (gtimer() - t0 > ns) return false;
   }
 }
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y,
-                                            int z, uint64_t* bar) {
+// One z-plane tile of grid b: a 4D tiled TMA load (x, y, z, b), no multicast.
+// Coordinates outside the tensor (halo beyond a face, z beyond a grid of the
+// batch) are filled with zeros by the copy engine.
+__device__ __forceinline__ void tma_load_plane(void* dst, const CUtensorMap* map, int x, int y,
+                                               int z, int b, uint64_t* bar) {
   asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes "
-      "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
-      "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(b), "r"(smem_u32(bar))
       : "memory");
 }
 
@@ -194,13 +200,16 @@ __device__ __forceinline__ void store_row(TS* p, const TA (&o)[V]) {
 // of consecutive items -- the same z chunk of neighbouring tiles -- and the
 // halo rows and columns that neighbouring tiles share are served by L2.
 struct Seg3D {
-  int64_t tile, za, zb;
+  int64_t tile, za, zb, b;
 };
 __device__ __forceinline__ Seg3D item_seg(int64_t it, const Work3D& w) {
   const int64_t ntiles = (int64_t)w.ntx * w.nty;
+  const int64_t nchunks = (w.nz + w.zc - 1) / w.zc;
   Seg3D s;
   s.tile = it % ntiles;
-  s.za = (it / ntiles) * w.zc;
+  const int64_t rest = it / ntiles;
+  s.za = (rest % nchunks) * w.zc;
+  s.b = rest / nchunks;
   s.zb = s.za + w.zc < w.nz ? s.za + w.zc : w.nz;
   return s;
 }
@@ -256,7 +265,7 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
         if (w.use_tma) {
           if (lane == 0) {
             mbar_expect_tx(&full[s], (unsigned)(XW * C::YW * sizeof(TS)));
-            tma_load_3d(slot, &map, gx, gy, (int)p, &full[s]);
+            tma_load_plane(slot, &map, gx, gy, (int)p, (int)sg.b, &full[s]);
           }
         } else {
           // plain loads for grids whose rows are not 16-byte multiples
@@ -265,7 +274,7 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
             const int64_t x = gx + c, y = gy + r;
             TS v = from_acc<TS>(TA(0));
             if (x >= 0 && x < nx && y >= 0 && y < ny && p >= 0 && p < nz)
-              v = src[p * nxy + y * nx + x];
+              v = src[(sg.b * nz + p) * nxy + y * nx + x];
             slot[r * XW + c] = v;
           }
           mbar_arrive(&full[s]);
@@ -405,17 +414,34 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
       for (int i = 0; i < PY; ++i) {
         const int64_t y = y0 + i;
         if (y >= ny || x0 >= nx) continue;
+        const int64_t cell = (sg.b * nz + z) * nxy + y * nx + x0;
+        constexpr int VB = V * (int)sizeof(TS);
+        const bool vec = x0 + V <= nx && ((uintptr_t)(dst + cell) % (VB >= 16 ? 16 : 8)) == 0;
         TA o[V];
 #pragma unroll
-        for (int j = 0; j < V; ++j) {
-          o[j] = acc[i][j];
-          if (any_ring) {
+        for (int j = 0; j < V; ++j) o[j] = acc[i][j];
+        if (w.rhs) {
+          // Jacobi form: out = stencil(in) + rhs_scale * rhs
+          const TS* fp = (const TS*)w.rhs + cell;
+          TA f[V];
+          if (vec && ((uintptr_t)fp % (VB >= 16 ? 16 : 8)) == 0) {
+            load_slot_row<TS, V>(f, fp);
+          } else {
+#pragma unroll
+            for (int j = 0; j < V; ++j) f[j] = x0 + j < nx ? to_acc(fp[j]) : TA(0);
+          }
+#pragma unroll
+          for (int j = 0; j < V; ++j) o[j] = fma((TA)w.rhs_scale, f[j], o[j]);
+        }
+        if (any_ring) {
+#pragma unroll
+          for (int j = 0; j < V; ++j) {
             const int64_t x = x0 + j;
             if (zring || y < R || y >= ny - R || x < R || x >= nx - R) o[j] = center[i][j];
           }
         }
-        TS* outp = dst + z * nxy + y * nx + x0;
-        if (x0 + V <= nx && ((uintptr_t)outp % (V * sizeof(TS) >= 16 ? 16 : 8)) == 0) {
+        TS* outp = dst + cell;
+        if (vec) {
           store_row<TS, V>(outp, o);
         } else {
 #pragma unroll

@@ -12,6 +12,7 @@ import numpy as np
 import pytest
 
 import oracle
+from ssam_b200.workloads import gaussian_rhs
 from ssam_cases import golden, rng, table2d, taps_j3d13pt, taps_j3d7pt
 
 DT = {"f32": np.float32, "f64": np.float64}
@@ -125,3 +126,24 @@ def test_clamp_boundary_equals_edge_padded_zero_conv():
     padded = np.pad(src, 1, mode="edge")
     want = oracle.conv2d(padded, filt, "zero")[1:-1, 1:-1]
     np.testing.assert_allclose(oracle.conv2d(src, filt, "clamp"), want, rtol=0, atol=1e-15)
+
+
+# ---- Poisson restatement (no reference code exists: checked by identities) --
+
+def test_poisson_residual_identity_and_jacobi_fixed_point():
+    g = rng(11)
+    u = g.standard_normal((2, 9, 9, 9))
+    # r = 0 - A u  =>  f := A u makes u the exact discrete solution
+    r, _ = oracle.residual7(np.zeros_like(u), u)
+    f = -r
+    _, rel = oracle.residual7(f, u)
+    assert rel.max() < 1e-13
+    # the exact solution is a fixed point of the Jacobi sweep
+    np.testing.assert_allclose(oracle.jacobi7(f, u, 3), u, rtol=0, atol=1e-12)
+
+
+def test_poisson_jacobi_reduces_residual():
+    f = gaussian_rhs(2, 12, 5)
+    u = oracle.jacobi7(f, np.zeros_like(f), 400)
+    _, rel = oracle.residual7(f, u)
+    assert rel.max() < 0.5

@@ -1,0 +1,51 @@
+"""The Poisson path: Jacobi sweeps (the 3D TMA stencil kernel with a
+right-hand side) and the FP64 residual against the FP64 oracle, and the
+defect-correction solve reaching its tolerance as judged by the oracle."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from ssam_b200.workloads import gaussian_rhs
+import ssam_b200 as S
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("dtype,rel", [(torch.float64, 1e-12), (torch.float32, 1e-5),
+                                       (torch.bfloat16, 2.0**-8)])
+@pytest.mark.parametrize("n,nb,sweeps", [(16, 3, 1), (16, 3, 2), (24, 2, 5), (17, 1, 3)])
+def test_jacobi_sweeps_vs_oracle(cuda, dtype, rel, n, nb, sweeps):
+    f = gaussian_rhs(nb, n, n * 10 + sweeps)
+    u0 = np.random.Generator(np.random.PCG64(n)).standard_normal(f.shape) * 1e-3
+    ft = torch.from_numpy(f).to(dtype).to(cuda)
+    ut = torch.from_numpy(u0).to(dtype).to(cuda)
+    got = S.poisson_jacobi(ft, ut, sweeps).double().cpu().numpy()
+    # the oracle sees the same rounded inputs
+    want = oracle.jacobi7(ft.double().cpu().numpy(), ut.double().cpu().numpy(), sweeps)
+    h2 = 1.0 / (n + 1) ** 2
+    scale = np.abs(want) + h2 * np.abs(f).max() / 6 + np.abs(u0).max()
+    err = np.abs(got - want) / scale
+    assert err.max() <= rel * sweeps, err.max()
+
+
+def test_residual_vs_oracle(cuda):
+    f = gaussian_rhs(3, 20, 1)
+    u = np.random.Generator(np.random.PCG64(2)).standard_normal(f.shape) * 1e-4
+    rel = S.poisson_residual(torch.from_numpy(f).to(cuda), torch.from_numpy(u).to(cuda))
+    _, want = oracle.residual7(f, u)
+    np.testing.assert_allclose(rel, want, rtol=1e-12)
+
+
+@pytest.mark.parametrize("sweep_dtype", ["f32", "bf16"])
+def test_defect_correction_reaches_tolerance(cuda, sweep_dtype):
+    n, nb = 24, 2
+    f = gaussian_rhs(nb, n, 7)
+    ft = torch.from_numpy(f).to(cuda)
+    u = torch.zeros_like(ft)
+    st = S.poisson_solve(ft, u, tol=1e-5, sweep_dtype=sweep_dtype, sweeps_per_correction=200,
+                         max_sweeps=20000)
+    assert st["converged"] == 1, st
+    assert st["rel_residual"] <= 1e-5
+    _, rel = oracle.residual7(f, u.cpu().numpy())
+    assert rel.max() <= 1.0001e-5, rel
