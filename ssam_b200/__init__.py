@@ -91,6 +91,10 @@ def _declare(lib):
     lib.ssam_poisson_residual.argtypes = [_vp, _vp, _int, _int, _dp, _vp]
     lib.ssam_poisson_jacobi.restype = _int
     lib.ssam_poisson_jacobi.argtypes = [_vp, _vp, _vp, _int, _int, _int, _int, _vp]
+    lib.ssam_cnn_conv3d.restype = _int
+    lib.ssam_cnn_conv3d.argtypes = [_vp, _vp, _vp, _vp, _int, _int, _int, ctypes.c_float, _vp]
+    lib.ssam_cnn_conv3d_wgrad.restype = _int
+    lib.ssam_cnn_conv3d_wgrad.argtypes = [_vp, _vp, _vp, _vp, _int, _int, _int, _vp]
     lib.ssam_autotune_stencil2d.restype = _int
     lib.ssam_autotune_stencil2d.argtypes = lib.ssam_stencil2d.argtypes + [_vp]
     for name in ("ssam_autotune_save", "ssam_autotune_load"):
@@ -365,3 +369,31 @@ def star_coeffs_from_matrix(m) -> list[float]:
     for k in range(1, r + 1):
         out += [rows[r - k][r], rows[r + k][r], rows[r][r - k], rows[r][r + k]]
     return out
+
+
+def cnn_conv3d(x0, weight, x1=None, dilation: int = 1, scale: float = 1.0, out=None,
+               stream=None):
+    """3x3x3 convolution of channels-last BF16 activations (nb, n, n, n, 16)
+    (x1: optional second 16-channel source) with weights (16, 27, 16 * nsrc)
+    on the tensor cores (``ssam_cnn_conv3d``)."""
+    import torch
+    nb, n = x0.shape[0], x0.shape[1]
+    if out is None:
+        out = torch.empty_like(x0)
+    _check(lib().ssam_cnn_conv3d(x0.data_ptr(), x1.data_ptr() if x1 is not None else None,
+                                 weight.data_ptr(), out.data_ptr(), nb, n, dilation, scale,
+                                 _stream_ptr(x0, stream)))
+    return out
+
+
+def cnn_conv3d_wgrad(x0, grad_out, x1=None, dilation: int = 1, stream=None):
+    """fp32 weight gradient (16, 27, 16 * nsrc) of ``cnn_conv3d``
+    (``ssam_cnn_conv3d_wgrad``)."""
+    import torch
+    nb, n = x0.shape[0], x0.shape[1]
+    nsrc = 2 if x1 is not None else 1
+    dw = torch.empty(16, 27, 16 * nsrc, dtype=torch.float32, device=x0.device)
+    _check(lib().ssam_cnn_conv3d_wgrad(x0.data_ptr(), x1.data_ptr() if x1 is not None else None,
+                                       grad_out.data_ptr(), dw.data_ptr(), nb, n, dilation,
+                                       _stream_ptr(x0, stream)))
+    return dw
