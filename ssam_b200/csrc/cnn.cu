@@ -133,7 +133,11 @@ constexpr int kWgStageVox = kWgStepVox * kWgStepsPerStage;
 constexpr int kWgAStep = 128 * kWgStepVox * 2;   // 4 KB
 constexpr int kWgBStep = 16 * kWgStepVox * 2;    // 512 B
 constexpr int kWgStages = 3;
-constexpr int kWgSmem = 128 + kWgStages * kWgStepsPerStage * (kWgAStep + kWgBStep) + 64;
+// (+32 KB guard: the MN-major A tiles span up to 16 MN groups x 2 K groups;
+// the guard keeps every address the descriptors can form inside the
+// allocation)
+constexpr int kWgSmem = 128 + kWgStages * kWgStepsPerStage * (kWgAStep + kWgBStep) + 64 +
+                        32 * 1024;
 
 template <int NSRC>
 __global__ void __launch_bounds__(128)
