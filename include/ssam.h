@@ -311,6 +311,8 @@ typedef struct ssam_poisson_options {
   int sweep_dtype;           /* SSAM_F32 or SSAM_BF16: storage of the Jacobi sweeps */
   int sweeps_per_correction; /* Jacobi sweeps between two FP64 residuals */
   int max_sweeps;            /* give up (converged = 0) after this many sweeps */
+  double omega;              /* Jacobi damping: u <- (1-w) u + w (nbrs + h^2 r) / 6;
+                                0 is taken as 1 (plain Jacobi) */
 } ssam_poisson_options;
 
 typedef struct ssam_poisson_stats {
@@ -319,6 +321,8 @@ typedef struct ssam_poisson_stats {
   int corrections;             /* FP64 defect-correction steps */
   double initial_rel_residual; /* max over the batch, for the initial guess */
   double rel_residual;         /* max over the batch, final (FP64) */
+  int cnn_corrections;         /* network corrections kept (learned solve only) */
+  int fell_back;               /* learned solve: the warm start was dropped for u = 0 */
 } ssam_poisson_stats;
 
 /*
@@ -331,6 +335,23 @@ typedef struct ssam_poisson_stats {
 SSAM_API int ssam_poisson_solve(const double* f, double* u, int n, int nbatch,
                                 const ssam_poisson_options* opt, ssam_poisson_stats* stats,
                                 void* stream);
+
+/*
+ * The learned arm: as ssam_poisson_solve, but each defect-correction step
+ * first applies the warm-start network `cnn` (ssam_cnn_create) to the FP64
+ * residual, u += CNN(r), and then runs the sweeps on the new residual (with
+ * u = 0 on entry the first step is the network's warm start).  A step with
+ * the network is kept only when it lowers the residual by 10% or more;
+ * otherwise u is restored and the rest of the solve is the plain method.  If
+ * the residual of the initial guess exceeds that of u = 0 the guess is
+ * replaced by zeros.  Damped sweeps (omega < 1) remove the high-frequency
+ * error that the network's BF16 arithmetic leaves.
+ * The network must have been created with nbatch_max >= nbatch and the same n.
+ * No counterpart in the reference (it has no Poisson solver).
+ */
+SSAM_API int ssam_poisson_solve_learned(const double* f, double* u, int n, int nbatch,
+                                        const ssam_poisson_options* opt, void* cnn,
+                                        ssam_poisson_stats* stats, void* stream);
 
 /* ||f - A u||_2 / ||f||_2 per right-hand side, in FP64 (`rel` is host, nbatch). */
 SSAM_API int ssam_poisson_residual(const double* f, const double* u, int n, int nbatch,
@@ -361,6 +382,31 @@ SSAM_API int ssam_cnn_conv3d(const void* in0, const void* in1, const void* weigh
 SSAM_API int ssam_cnn_conv3d_wgrad(const void* in0, const void* in1, const void* grad_out,
                                    float* dweight, int nbatch, int n, int dilation,
                                    void* stream);
+
+/*
+ * The warm-start network for the Poisson solve on n^3 grids (n a power of two
+ * >= 32): a 3-level, 16-channel linear U-Net of the convolutions above
+ * (levels n, n/2, n/4; dilations 1, 2, 4, 8 at the bottom), trained and run
+ * on the GPU.  f and u are FP64 (nbatch, n, n, n) device arrays.
+ */
+SSAM_API int ssam_cnn_create(int n, int nbatch_max, unsigned long long seed, void** handle);
+SSAM_API int ssam_cnn_destroy(void* handle);
+SSAM_API int ssam_cnn_num_params(void* handle, int64_t* count);
+/* fp32 parameters / last gradient to host arrays of ssam_cnn_num_params (either may be NULL) */
+SSAM_API int ssam_cnn_get_params(void* handle, float* host_params, float* host_grads);
+SSAM_API int ssam_cnn_set_params(void* handle, const float* host_params);
+/* u0 = network(f): the warm start */
+SSAM_API int ssam_cnn_forward(void* handle, const double* f, double* u0, int nbatch,
+                              void* stream);
+/* forward + backward of the mean squared error against `target` (normalised
+ * by the input's RMS); `loss` (host) receives it.  Synchronous. */
+SSAM_API int ssam_cnn_gradient(void* handle, const double* f, const double* target, int nbatch,
+                               double* loss, void* stream);
+/* one Adam step (beta 0.9 / 0.999) with the last gradient */
+SSAM_API int ssam_cnn_adam_step(void* handle, float lr, void* stream);
+/* weights as a one-line JSON header + float32 blob */
+SSAM_API int ssam_cnn_save(void* handle, const char* path);
+SSAM_API int ssam_cnn_load(void* handle, const char* path);
 
 /*
  * Synchronises `stream` and reports whether a bounded device-side wait of

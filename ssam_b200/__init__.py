@@ -47,14 +47,16 @@ BATCH_PERSISTENT, BATCH_PER_GRID = 0, 1
 class PoissonOptions(ctypes.Structure):
     """``ssam_poisson_options``."""
     _fields_ = [("tol", ctypes.c_double), ("sweep_dtype", ctypes.c_int),
-                ("sweeps_per_correction", ctypes.c_int), ("max_sweeps", ctypes.c_int)]
+                ("sweeps_per_correction", ctypes.c_int), ("max_sweeps", ctypes.c_int),
+                ("omega", ctypes.c_double)]
 
 
 class PoissonStats(ctypes.Structure):
     """``ssam_poisson_stats``."""
     _fields_ = [("converged", ctypes.c_int), ("sweeps", ctypes.c_int),
                 ("corrections", ctypes.c_int), ("initial_rel_residual", ctypes.c_double),
-                ("rel_residual", ctypes.c_double)]
+                ("rel_residual", ctypes.c_double), ("cnn_corrections", ctypes.c_int),
+                ("fell_back", ctypes.c_int)]
 
 _i64 = ctypes.c_int64
 _int = ctypes.c_int
@@ -87,6 +89,10 @@ def _declare(lib):
     lib.ssam_poisson_solve.restype = _int
     lib.ssam_poisson_solve.argtypes = [_vp, _vp, _int, _int, ctypes.POINTER(PoissonOptions),
                                        ctypes.POINTER(PoissonStats), _vp]
+    lib.ssam_poisson_solve_learned.restype = _int
+    lib.ssam_poisson_solve_learned.argtypes = [_vp, _vp, _int, _int,
+                                               ctypes.POINTER(PoissonOptions), _vp,
+                                               ctypes.POINTER(PoissonStats), _vp]
     lib.ssam_poisson_residual.restype = _int
     lib.ssam_poisson_residual.argtypes = [_vp, _vp, _int, _int, _dp, _vp]
     lib.ssam_poisson_jacobi.restype = _int
@@ -95,6 +101,19 @@ def _declare(lib):
     lib.ssam_cnn_conv3d.argtypes = [_vp, _vp, _vp, _vp, _int, _int, _int, ctypes.c_float, _vp]
     lib.ssam_cnn_conv3d_wgrad.restype = _int
     lib.ssam_cnn_conv3d_wgrad.argtypes = [_vp, _vp, _vp, _vp, _int, _int, _int, _vp]
+    for name, args in (("ssam_cnn_create", [_int, _int, ctypes.c_ulonglong,
+                                             ctypes.POINTER(ctypes.c_void_p)]),
+                       ("ssam_cnn_destroy", [_vp]),
+                       ("ssam_cnn_num_params", [_vp, ctypes.POINTER(ctypes.c_int64)]),
+                       ("ssam_cnn_get_params", [_vp, _vp, _vp]),
+                       ("ssam_cnn_set_params", [_vp, _vp]),
+                       ("ssam_cnn_forward", [_vp, _vp, _vp, _int, _vp]),
+                       ("ssam_cnn_gradient", [_vp, _vp, _vp, _int, _dp, _vp]),
+                       ("ssam_cnn_adam_step", [_vp, ctypes.c_float, _vp]),
+                       ("ssam_cnn_save", [_vp, ctypes.c_char_p]),
+                       ("ssam_cnn_load", [_vp, ctypes.c_char_p])):
+        getattr(lib, name).restype = _int
+        getattr(lib, name).argtypes = args
     lib.ssam_autotune_stencil2d.restype = _int
     lib.ssam_autotune_stencil2d.argtypes = lib.ssam_stencil2d.argtypes + [_vp]
     for name in ("ssam_autotune_save", "ssam_autotune_load"):
@@ -289,18 +308,26 @@ def _poisson_grid(t):
 
 
 def poisson_solve(f, u, tol: float = 1e-5, sweep_dtype=None, sweeps_per_correction: int = 1000,
-                  max_sweeps: int = 200000, stream=None) -> dict:
+                  max_sweeps: int = 200000, cnn=None, omega: float = 1.0,
+                  stream=None) -> dict:
     """``ssam_poisson_solve``: f, u are float64 (nbatch, n, n, n); u holds the
-    initial guess and receives the solution."""
+    initial guess and receives the solution.  With ``cnn`` (a WarmStartCNN)
+    this is ``ssam_poisson_solve_learned``: the network's correction comes
+    before the sweeps of every defect-correction step."""
     import torch
     nb, n = _poisson_grid(f)
     if u.shape != f.shape or f.dtype != torch.float64 or u.dtype != torch.float64:
         raise ValueError("f and u must be float64 tensors of the same shape")
     dt = F32 if sweep_dtype in (None, "f32", torch.float32) else BF16
-    opt = PoissonOptions(tol, dt, sweeps_per_correction, max_sweeps)
+    opt = PoissonOptions(tol, dt, sweeps_per_correction, max_sweeps, omega)
     st = PoissonStats()
-    _check(lib().ssam_poisson_solve(f.data_ptr(), u.data_ptr(), n, nb, ctypes.byref(opt),
-                                    ctypes.byref(st), _stream_ptr(f, stream)))
+    if cnn is None:
+        _check(lib().ssam_poisson_solve(f.data_ptr(), u.data_ptr(), n, nb, ctypes.byref(opt),
+                                        ctypes.byref(st), _stream_ptr(f, stream)))
+    else:
+        _check(lib().ssam_poisson_solve_learned(f.data_ptr(), u.data_ptr(), n, nb,
+                                                ctypes.byref(opt), cnn._h, ctypes.byref(st),
+                                                _stream_ptr(f, stream)))
     return {k: getattr(st, k) for k, _ in st._fields_}
 
 
@@ -397,3 +424,67 @@ def cnn_conv3d_wgrad(x0, grad_out, x1=None, dilation: int = 1, stream=None):
                                        grad_out.data_ptr(), dw.data_ptr(), nb, n, dilation,
                                        _stream_ptr(x0, stream)))
     return dw
+
+
+class WarmStartCNN:
+    """The Poisson warm-start network (``ssam_cnn_*``): a 3-level, 16-channel
+    linear U-Net on the tensor cores.  f and u are float64 CUDA tensors of
+    shape (nbatch, n, n, n)."""
+
+    def __init__(self, n: int, nbatch_max: int, seed: int = 0):
+        self.n, self.nbatch_max = n, nbatch_max
+        h = ctypes.c_void_p()
+        _check(lib().ssam_cnn_create(n, nbatch_max, seed, ctypes.byref(h)))
+        self._h = h
+        cnt = ctypes.c_int64()
+        _check(lib().ssam_cnn_num_params(self._h, ctypes.byref(cnt)))
+        self.num_params = cnt.value
+
+    def close(self):
+        if self._h:
+            lib().ssam_cnn_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def forward(self, f, out=None, stream=None):
+        import torch
+        if out is None:
+            out = torch.empty_like(f)
+        _check(lib().ssam_cnn_forward(self._h, f.data_ptr(), out.data_ptr(), f.shape[0],
+                                      _stream_ptr(f, stream)))
+        return out
+
+    def gradient(self, f, target, stream=None) -> float:
+        loss = ctypes.c_double()
+        _check(lib().ssam_cnn_gradient(self._h, f.data_ptr(), target.data_ptr(), f.shape[0],
+                                       ctypes.byref(loss), _stream_ptr(f, stream)))
+        return loss.value
+
+    def adam_step(self, lr: float, stream=None):
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream()
+        _check(lib().ssam_cnn_adam_step(self._h, lr, ctypes.c_void_p(s.cuda_stream)))
+
+    def params(self):
+        import numpy as np
+        w = np.empty(self.num_params, np.float32)
+        g = np.empty(self.num_params, np.float32)
+        _check(lib().ssam_cnn_get_params(self._h, w.ctypes.data_as(_vp), g.ctypes.data_as(_vp)))
+        return w, g
+
+    def set_params(self, w):
+        import numpy as np
+        w = np.ascontiguousarray(w, np.float32)
+        assert w.size == self.num_params
+        _check(lib().ssam_cnn_set_params(self._h, w.ctypes.data_as(_vp)))
+
+    def save(self, path: str):
+        _check(lib().ssam_cnn_save(self._h, path.encode()))
+
+    def load(self, path: str):
+        _check(lib().ssam_cnn_load(self._h, path.encode()))

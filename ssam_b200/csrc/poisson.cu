@@ -36,7 +36,7 @@ constexpr int kResidualThreads = 256;
 template <typename TS>
 __global__ void __launch_bounds__(kResidualThreads)
 residual_kernel(const double* __restrict__ u, const double* __restrict__ f, TS* __restrict__ r_lp,
-                double* __restrict__ partials, int n, double inv_h2) {
+                double* __restrict__ r64, double* __restrict__ partials, int n, double inv_h2) {
   const int b = blockIdx.y;
   const int64_t n3 = (int64_t)n * n * n, nn = (int64_t)n * n;
   const double* ub = u + b * n3;
@@ -56,6 +56,7 @@ residual_kernel(const double* __restrict__ u, const double* __restrict__ f, TS* 
     const double fc = fb[c];
     const double r = fc - (6.0 * uc - nb) * inv_h2;
     if (r_lp) r_lp[b * n3 + c] = from_acc<TS>((typename Traits<TS>::TA)r);
+    if (r64) r64[b * n3 + c] = r;
     rr += r * r;
     ff += fc * fc;
   }
@@ -102,6 +103,13 @@ __global__ void add_correction_kernel(double* __restrict__ u, const TS* __restri
     u[i] += (double)to_acc(e[i]);
 }
 
+__global__ void axpy_kernel(double* __restrict__ u, const double* __restrict__ c, double a,
+                            int64_t count) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+       i += (int64_t)gridDim.x * blockDim.x)
+    u[i] += a * c[i];
+}
+
 int sm_count() {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
@@ -115,15 +123,15 @@ int sm_count() {
 // 2 per grid); optionally r in low precision.  Synchronises the stream.
 static int residual(const double* f, const double* u, void* r_lp, int lp_dtype, int n, int nb,
                     double* partials, int blocks, double* d_norms, double* norms2,
-                    cudaStream_t s) {
+                    cudaStream_t s, double* r64 = nullptr) {
   const double h = 1.0 / (n + 1);
   dim3 grid(blocks, nb);
   if (lp_dtype == SSAM_BF16)
     residual_kernel<__nv_bfloat16><<<grid, kResidualThreads, 0, s>>>(
-        u, f, (__nv_bfloat16*)r_lp, partials, n, 1.0 / (h * h));
+        u, f, (__nv_bfloat16*)r_lp, r64, partials, n, 1.0 / (h * h));
   else
-    residual_kernel<float><<<grid, kResidualThreads, 0, s>>>(u, f, (float*)r_lp, partials, n,
-                                                             1.0 / (h * h));
+    residual_kernel<float><<<grid, kResidualThreads, 0, s>>>(u, f, (float*)r_lp, r64, partials,
+                                                             n, 1.0 / (h * h));
   count_launch();
   norms_kernel<<<(nb + 127) / 128, 128, 0, s>>>(partials, blocks, nb, d_norms);
   count_launch();
@@ -134,26 +142,28 @@ static int residual(const double* f, const double* u, void* r_lp, int lp_dtype, 
   return SSAM_OK;
 }
 
-// The Jacobi coefficient cube: neighbours 1/6, centre 0.
-static void jacobi_cube(double* cube) {
+// The (damped) Jacobi coefficient cube: neighbours omega/6, centre 1-omega.
+static void jacobi_cube(double* cube, double omega = 1.0) {
   for (int i = 0; i < 27; ++i) cube[i] = 0.0;
-  const double w = 1.0 / 6.0;
+  cube[13] = 1.0 - omega;
+  const double w = omega / 6.0;
   cube[0 * 9 + 1 * 3 + 1] = cube[2 * 9 + 1 * 3 + 1] = w;
   cube[1 * 9 + 0 * 3 + 1] = cube[1 * 9 + 2 * 3 + 1] = w;
   cube[1 * 9 + 1 * 3 + 0] = cube[1 * 9 + 1 * 3 + 2] = w;
 }
 
-// `sweeps` Jacobi sweeps u <- (nbrs(u) + h^2 rhs) / 6 from u_in; the result is
-// in u_out.  `tmp` is a second grid for the ping-pong (may alias nothing).
+// `sweeps` Jacobi sweeps u <- (1-omega) u + omega (nbrs(u) + h^2 rhs) / 6
+// from u_in; the result is in u_out.  `tmp` is a second grid for the
+// ping-pong (may alias nothing).
 static int jacobi_chain(const void* rhs, const void* u_in, void* u_out, void* tmp, int n, int nb,
-                        int dtype, int sweeps, cudaStream_t s) {
+                        int dtype, int sweeps, cudaStream_t s, double omega = 1.0) {
   double cube[27];
-  jacobi_cube(cube);
+  jacobi_cube(cube, omega);
   const double h = 1.0 / (n + 1);
   const void* in = u_in;
   for (int k = 0; k < sweeps; ++k) {
     void* out = ((sweeps - 1 - k) % 2 == 0) ? u_out : tmp;
-    int st = sweep_3d(in, out, n, nb, dtype, cube, rhs, h * h / 6.0, s);
+    int st = sweep_3d(in, out, n, nb, dtype, cube, rhs, omega * h * h / 6.0, s);
     if (st != SSAM_OK) return st;
     in = out;
   }
@@ -208,15 +218,31 @@ extern "C" int ssam_poisson_residual(const double* f, const double* u, int n, in
   return SSAM_OK;
 }
 
-extern "C" int ssam_poisson_solve(const double* f, double* u, int n, int nbatch,
-                                  const ssam_poisson_options* opt, ssam_poisson_stats* stats,
-                                  void* stream) {
+namespace ssam {
+int cnn_check(void* cnn, int n, int nbatch);
+int cnn_apply(void* cnn, const double* r, double* c, int nbatch, cudaStream_t s);
+}
+
+// Defect-correction solve; with `cnn`, every correction first adds the
+// network's approximate solve of A c = r to u in FP64, then runs the
+// low-precision sweeps on the new residual.  A network cycle is kept when the
+// next residual is below 0.9 times the one before it; otherwise u is restored
+// and the network is not used again in this solve.
+static int poisson_solve(const double* f, double* u, int n, int nbatch,
+                         const ssam_poisson_options* opt, void* cnn, ssam_poisson_stats* stats,
+                         cudaStream_t stream) {
   if (!f || !u || !opt) return fail(SSAM_ERR_INVALID, "NULL pointer");
   if (n < 1 || nbatch < 1) return fail(SSAM_ERR_INVALID, "bad n/nbatch");
   if (opt->sweep_dtype != SSAM_F32 && opt->sweep_dtype != SSAM_BF16)
     return fail(SSAM_ERR_INVALID, "sweep_dtype must be SSAM_F32 or SSAM_BF16");
   if (opt->sweeps_per_correction < 1 || opt->max_sweeps < 0 || !(opt->tol > 0))
     return fail(SSAM_ERR_INVALID, "bad tol / sweeps_per_correction / max_sweeps");
+  const double omega = opt->omega == 0.0 ? 1.0 : opt->omega;
+  if (!(omega > 0.0 && omega <= 1.0)) return fail(SSAM_ERR_INVALID, "omega must be in (0, 1]");
+  if (cnn) {
+    const int cs = cnn_check(cnn, n, nbatch);
+    if (cs != SSAM_OK) return cs;
+  }
   cudaStream_t s = (cudaStream_t)stream;
   const int dt = opt->sweep_dtype;
   const size_t cells = (size_t)n * n * n * nbatch;
@@ -225,8 +251,9 @@ extern "C" int ssam_poisson_solve(const double* f, double* u, int n, int nbatch,
   const size_t pbytes = sizeof(double) * 2 * ((size_t)blocks * nbatch + nbatch);
   // one allocation: r (low precision), e and its ping-pong partner, partial sums
   const size_t lp_al = (lp + 255) / 256 * 256;
+  const size_t f64_al = (cells * sizeof(double) + 255) / 256 * 256;
   void* work = nullptr;
-  int st = scratch_alloc(&work, 3 * lp_al + pbytes, s);
+  int st = scratch_alloc(&work, 3 * lp_al + pbytes + (cnn ? 3 * f64_al : 0), s);
   if (st != SSAM_OK) return st;
   char* w8 = (char*)work;
   void* r_lp = w8;
@@ -234,7 +261,16 @@ extern "C" int ssam_poisson_solve(const double* f, double* u, int n, int nbatch,
   void* e_tmp = w8 + 2 * lp_al;
   double* partials = (double*)(w8 + 3 * lp_al);
   double* d_norms = partials + 2 * (size_t)blocks * nbatch;
+  // the learned solve: r in FP64 (network input), the network's correction,
+  // and u before the last network cycle (restored if that cycle did not pay)
+  double* r64 = cnn ? (double*)(w8 + 3 * lp_al + pbytes) : nullptr;
+  double* c64 = cnn ? (double*)(w8 + 3 * lp_al + pbytes + f64_al) : nullptr;
+  double* u_save = cnn ? (double*)(w8 + 3 * lp_al + pbytes + 2 * f64_al) : nullptr;
   std::vector<double> norms2(2 * nbatch);
+  bool use_cnn = cnn != nullptr;
+  bool first = true;
+  bool judge_cnn = false;  // the last cycle used the network
+  double before_cnn = 0.0;
 
   ssam_poisson_stats local = {};
   ssam_poisson_stats* out = stats ? stats : &local;
@@ -243,21 +279,74 @@ extern "C" int ssam_poisson_solve(const double* f, double* u, int n, int nbatch,
   cudaGraphExec_t chain = nullptr;
   const size_t nthreads = 256;
   const int cblocks = (int)std::min<size_t>((cells + nthreads - 1) / nthreads, 148 * 16);
+  auto worst_rel = [&]() {
+    double m = 0.0;
+    for (int b = 0; b < nbatch; ++b)
+      m = std::max(m, norms2[2 * b + 1] > 0 ? sqrt(norms2[2 * b] / norms2[2 * b + 1]) : 0.0);
+    return m;
+  };
   while (true) {
-    st = residual(f, u, r_lp, dt, n, nbatch, partials, blocks, d_norms, norms2.data(), s);
+    st = residual(f, u, r_lp, dt, n, nbatch, partials, blocks, d_norms, norms2.data(), s,
+                  use_cnn ? r64 : nullptr);
     if (st != SSAM_OK) break;
-    worst = 0.0;
-    for (int b = 0; b < nbatch; ++b) {
-      const double rel = norms2[2 * b + 1] > 0 ? sqrt(norms2[2 * b] / norms2[2 * b + 1]) : 0.0;
-      worst = std::max(worst, rel);
+    worst = worst_rel();
+    if (first) {
+      first = false;
+      out->initial_rel_residual = worst;
+      if (cnn && worst > 1.0) {
+        // the initial guess is worse than no guess at all: start from u = 0
+        cudaError_t ce = cudaMemsetAsync(u, 0, cells * sizeof(double), s);
+        if (ce != cudaSuccess) {
+          st = fail_cuda(ce, "cudaMemsetAsync(u)");
+          break;
+        }
+        out->fell_back = 1;
+        first = true;
+        continue;
+      }
     }
-    if (out->corrections == 0) out->initial_rel_residual = worst;
+    if (judge_cnn) {
+      judge_cnn = false;
+      if (worst < 0.9 * before_cnn) {
+        out->cnn_corrections += 1;
+      } else {
+        // the network's cycle did not lower the residual enough: undo it and
+        // go on with plain cycles
+        use_cnn = false;
+        cudaError_t ce =
+            cudaMemcpyAsync(u, u_save, cells * sizeof(double), cudaMemcpyDeviceToDevice, s);
+        if (ce != cudaSuccess) {
+          st = fail_cuda(ce, "restoring u");
+          break;
+        }
+        st = residual(f, u, r_lp, dt, n, nbatch, partials, blocks, d_norms, norms2.data(), s);
+        if (st != SSAM_OK) break;
+        worst = worst_rel();
+      }
+    }
     out->rel_residual = worst;
     if (worst <= opt->tol) {
       out->converged = 1;
       break;
     }
     if (out->sweeps >= opt->max_sweeps) break;
+    if (use_cnn) {
+      // u += network(r), then the sweeps below smooth what the network left
+      cudaError_t ce =
+          cudaMemcpyAsync(u_save, u, cells * sizeof(double), cudaMemcpyDeviceToDevice, s);
+      if (ce != cudaSuccess) {
+        st = fail_cuda(ce, "saving u");
+        break;
+      }
+      before_cnn = worst;
+      judge_cnn = true;
+      st = cnn_apply(cnn, r64, c64, nbatch, s);
+      if (st != SSAM_OK) break;
+      axpy_kernel<<<cblocks, nthreads, 0, s>>>(u, c64, 1.0, (int64_t)cells);
+      count_launch();
+      st = residual(f, u, r_lp, dt, n, nbatch, partials, blocks, d_norms, norms2.data(), s);
+      if (st != SSAM_OK) break;
+    }
     const int k = std::min(opt->sweeps_per_correction, opt->max_sweeps - out->sweeps);
     // e = k Jacobi sweeps on A e = r from e = 0; the chain (memset + k sweeps)
     // is captured once and replayed for every correction of this size
@@ -286,7 +375,8 @@ extern "C" int ssam_poisson_solve(const double* f, double* u, int n, int nbatch,
         // zero start grid is the other one, so no launch reads what it writes
         void* zero_src = (k % 2 == 1) ? e_tmp : e;
         if (ce == cudaSuccess) ce = cudaMemsetAsync(zero_src, 0, lp, cs);
-        if (ce == cudaSuccess) st = jacobi_chain(r_lp, zero_src, e, e_tmp, n, nbatch, dt, k, cs);
+        if (ce == cudaSuccess)
+          st = jacobi_chain(r_lp, zero_src, e, e_tmp, n, nbatch, dt, k, cs, omega);
         cudaError_t ee = cudaStreamEndCapture(cs, &g);
         if (ce == cudaSuccess) ce = ee;
         if (ce == cudaSuccess && st == SSAM_OK) ce = cudaGraphInstantiate(&chain, g, 0);
@@ -321,3 +411,20 @@ extern "C" int ssam_poisson_solve(const double* f, double* u, int n, int nbatch,
   scratch_free(work, s);
   return st;
 }
+
+extern "C" {
+
+int ssam_poisson_solve(const double* f, double* u, int n, int nbatch,
+                       const ssam_poisson_options* opt, ssam_poisson_stats* stats,
+                       void* stream) {
+  return poisson_solve(f, u, n, nbatch, opt, nullptr, stats, (cudaStream_t)stream);
+}
+
+int ssam_poisson_solve_learned(const double* f, double* u, int n, int nbatch,
+                               const ssam_poisson_options* opt, void* cnn,
+                               ssam_poisson_stats* stats, void* stream) {
+  if (!cnn) return fail(SSAM_ERR_INVALID, "cnn handle must not be NULL");
+  return poisson_solve(f, u, n, nbatch, opt, cnn, stats, (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -66,3 +66,101 @@ def test_conv3d_weight_grad_vs_torch_autograd(cuda, nsrc, n, dil):
     mag = torch.stack([wa.grad[:, :, kz, ky, kx] for kz, ky, kx in TAPS], dim=1)
     err = (dw - want).abs() - 1e-4 * mag
     assert err.max().item() <= 0, f"max excess {err.max().item()}"
+
+
+# ---- the whole network: forward and gradient against a float64 CPU mirror --
+
+LAYERS = [  # (level, nsrc, dilation) in parameter order
+    (0, 1, 1), (0, 1, 1), (1, 1, 1), (1, 1, 1), (2, 1, 1), (2, 1, 2), (2, 1, 4), (2, 1, 8),
+    (1, 2, 1), (1, 1, 1), (0, 2, 1), (0, 1, 1)]
+OUT_SCALE = 0.03
+
+
+def mirror_loss(params, f, target=None):
+    """The network in float64 torch (channels-first); returns (u0, loss)."""
+    ws, off = [], 0
+    for lvl, nsrc, dil in LAYERS:
+        cnt = 16 * 27 * 16 * nsrc
+        ws.append(to_torch_weight(params[off:off + cnt].view(16, 27, 16 * nsrc)))
+        off += cnt
+    wh = params[off:off + 16]
+    nb, n = f.shape[0], f.shape[1]
+    rms = f.pow(2).mean(dim=(1, 2, 3)).sqrt()
+    x = torch.zeros(nb, 16, n, n, n, dtype=torch.float64)
+    x[:, 0] = f / rms.view(-1, 1, 1, 1)
+
+    def conv(i, *xs):
+        return F.conv3d(torch.cat(xs, 1), ws[i], padding=LAYERS[i][2], dilation=LAYERS[i][2])
+
+    a1 = conv(0, x)
+    s1 = conv(1, a1)
+    p1 = F.avg_pool3d(s1, 2)
+    a2 = conv(2, p1)
+    s2 = conv(3, a2)
+    p2 = F.avg_pool3d(s2, 2)
+    b = conv(7, conv(6, conv(5, conv(4, p2))))
+    u2 = F.interpolate(b, scale_factor=2, mode="nearest")
+    d2 = conv(9, conv(8, u2, s2))
+    u1 = F.interpolate(d2, scale_factor=2, mode="nearest")
+    d1 = conv(11, conv(10, u1, s1))
+    y = (d1 * wh.view(1, 16, 1, 1, 1)).sum(1)
+    scale = (rms * OUT_SCALE).view(-1, 1, 1, 1)
+    u0 = y * scale
+    loss = None
+    if target is not None:
+        loss = ((y - target / scale) ** 2).mean()
+    return u0, loss
+
+
+def test_cnn_forward_and_gradient_vs_float64_mirror(cuda):
+    from ssam_b200.workloads import gaussian_rhs
+    n, nb = 32, 2
+    net = S.WarmStartCNN(n, nb, seed=3)
+    f = torch.from_numpy(gaussian_rhs(nb, n, 11))
+    target = torch.from_numpy(gaussian_rhs(nb, n, 12)) * 0.01
+    w, _ = net.params()
+    # the mirror uses the BF16-rounded conv weights the GPU multiplies with
+    pw = torch.from_numpy(w).double()
+    nconv = net.num_params - 16
+    pw[:nconv] = pw[:nconv].to(torch.bfloat16).double()
+    pw.requires_grad_(True)
+    u_ref, loss_ref = mirror_loss(pw, f, target)
+    loss_ref.backward()
+    u_gpu = net.forward(f.to(cuda)).cpu()
+    rel_u = ((u_gpu - u_ref.detach()).norm() / u_ref.detach().norm()).item()
+    assert rel_u < 3e-2, rel_u
+    loss = net.gradient(f.to(cuda), target.to(cuda))
+    assert abs(loss - loss_ref.item()) <= 3e-2 * loss_ref.item()
+    _, g = net.params()
+    g_ref = pw.grad.numpy()
+    off = 0
+    for i, (_, nsrc, _) in enumerate(LAYERS + [(0, 0, 0)]):
+        cnt = 16 * 27 * 16 * nsrc if i < len(LAYERS) else 16
+        a, b = g[off:off + cnt], g_ref[off:off + cnt]
+        rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+        assert rel < 5e-2, f"layer {i}: relative gradient error {rel:.3e}"
+        off += cnt
+    net.close()
+
+
+def test_cnn_training_reduces_loss_and_roundtrips(cuda, tmp_path):
+    from ssam_b200.workloads import gaussian_rhs
+    n, nb = 32, 4
+    net = S.WarmStartCNN(n, nb, seed=5)
+    f = torch.from_numpy(gaussian_rhs(nb, n, 21)).to(cuda)
+    u = torch.zeros_like(f)
+    S.poisson_solve(f, u, tol=1e-6, sweeps_per_correction=500, max_sweeps=50000)
+    first = net.gradient(f, u)
+    for _ in range(60):
+        net.gradient(f, u)
+        net.adam_step(3e-3)
+    last = net.gradient(f, u)
+    assert last < 0.6 * first, (first, last)
+    p = str(tmp_path / "net.bin")
+    net.save(p)
+    u1 = net.forward(f).clone()
+    other = S.WarmStartCNN(n, nb, seed=99)
+    other.load(p)
+    assert torch.equal(other.forward(f), u1)
+    net.close()
+    other.close()

@@ -49,3 +49,27 @@ def test_defect_correction_reaches_tolerance(cuda, sweep_dtype):
     assert st["rel_residual"] <= 1e-5
     _, rel = oracle.residual7(f, u.cpu().numpy())
     assert rel.max() <= 1.0001e-5, rel
+
+
+def test_learned_solve_with_untrained_network_falls_back_and_converges(cuda):
+    """A random network's corrections do not lower the residual: the solve
+    rejects them, turns the network off and still reaches the tolerance."""
+    n, nb = 32, 2
+    f = gaussian_rhs(nb, n, 8)
+    ft = torch.from_numpy(f).to(cuda)
+    net = S.WarmStartCNN(n, nb, seed=3)
+    u = torch.zeros_like(ft)
+    st = S.poisson_solve(ft, u, tol=1e-5, sweep_dtype="bf16", sweeps_per_correction=300,
+                         max_sweeps=40000, cnn=net)
+    assert st["converged"] == 1, st
+    _, rel = oracle.residual7(f, u.cpu().numpy())
+    assert rel.max() <= 1.0001e-5, rel
+
+
+def test_learned_solve_rejects_bad_arguments(cuda):
+    n = 32
+    ft = torch.from_numpy(gaussian_rhs(2, n, 1)).to(cuda)
+    for net in (S.WarmStartCNN(64, 2, seed=0), S.WarmStartCNN(n, 1, seed=0)):
+        with pytest.raises(S.SsamError):  # built for another n / fewer right-hand sides
+            S.poisson_solve(ft, torch.zeros_like(ft), cnn=net)
+        net.close()
