@@ -14,6 +14,8 @@
 // a shared-memory stage, one thread issues a 128x16x16 tcgen05.mma into TMEM,
 // and a tcgen05.commit on the stage's mbarrier frees it for reuse four steps
 // later.  The epilogue reads the accumulators with tcgen05.ld and stores BF16.
+#include <stdlib.h>
+
 #include <algorithm>
 #include <string>
 #include <vector>
@@ -273,8 +275,27 @@ int log2_exact(int n) {
 
 // out = conv3d(in0 (+ in1 as channels 16..31), w) * out_scale over nb grids of
 // n^3 (n a power of two, n^3 a multiple of 128).
+int conv3d_fwd_tma(const void* in0, const void* in1, const void* w, void* out, int nb, int n,
+                   int dil, float out_scale, cudaStream_t s);
+
+// SSAM_CONV_GATHER=1 in the environment forces the gather kernel (to check
+// it against the same oracle as the TMA kernel).
+static bool force_gather() {
+  static const bool v = [] {
+    const char* e = getenv("SSAM_CONV_GATHER");
+    return e && e[0] == '1';
+  }();
+  return v;
+}
+
 int conv3d_fwd(const void* in0, const void* in1, const void* w, void* out, int nb, int n,
                int dil, float out_scale, cudaStream_t s) {
+  if (in0 && w && out &&
+      ((uintptr_t)in0 | (uintptr_t)w | (uintptr_t)out | (uintptr_t)in1) % 16 == 0 &&
+      !force_gather()) {
+    const int st = conv3d_fwd_tma(in0, in1, w, out, nb, n, dil, out_scale, s);
+    if (st != SSAM_ERR_UNSUPPORTED) return st;
+  }
   const int l2 = log2_exact(n);
   if (l2 < 0 || (int64_t)n * n * n % kTile != 0)
     return fail(SSAM_ERR_INVALID, "conv3d: n must be a power of two with n^3 % 128 == 0");
@@ -357,8 +378,7 @@ extern "C" int ssam_cnn_conv3d_wgrad(const void* in0, const void* in1, const voi
                                      float* dweight, int nbatch, int n, int dilation,
                                      void* stream) {
   if (!in0 || !grad_out || !dweight) return fail(SSAM_ERR_INVALID, "wgrad: NULL tensor");
-  if (nbatch < 1 || dilation < 1 || dilation >= n)
-    return fail(SSAM_ERR_INVALID, "wgrad: bad nbatch / dilation");
+  if (nbatch < 1 || dilation < 1) return fail(SSAM_ERR_INVALID, "wgrad: bad nbatch / dilation");
   cudaStream_t s = (cudaStream_t)stream;
   const int64_t nvox = (int64_t)nbatch * n * n * n;
   const int64_t slabs = conv3d_wgrad_slabs(nvox);
@@ -372,7 +392,6 @@ extern "C" int ssam_cnn_conv3d_wgrad(const void* in0, const void* in1, const voi
 
 extern "C" int ssam_cnn_conv3d(const void* in0, const void* in1, const void* weight, void* out,
                                int nbatch, int n, int dilation, float out_scale, void* stream) {
-  if (nbatch < 1 || dilation < 1 || dilation >= n)
-    return fail(SSAM_ERR_INVALID, "conv3d: bad nbatch / dilation");
+  if (nbatch < 1 || dilation < 1) return fail(SSAM_ERR_INVALID, "conv3d: bad nbatch / dilation");
   return conv3d_fwd(in0, in1, weight, out, nbatch, n, dilation, out_scale, (cudaStream_t)stream);
 }

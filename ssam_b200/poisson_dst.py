@@ -40,3 +40,31 @@ def solve(f):
     for d in (1, 2, 3):
         t = _dst1(t, d)
     return t / (2.0 * (n + 1)) ** 3
+
+
+def random_spectrum_rhs(nb: int, n: int, seed: int, device="cuda"):
+    """Right-hand sides whose solutions have random sine-mode spectra with a
+    power-law fall-off |k|^-alpha, alpha ~ U[1, 3] per sample (from rough to
+    smooth solutions); unit RMS.  f = A e for e = DST^-1 of the random
+    coefficients, computed in the spectral domain.  Broadens the training set
+    beyond Gaussian bumps so the network's A^-1 holds across frequency bands
+    (the inputs it meets inside defect correction are residuals, not bumps)."""
+    import torch
+    g = torch.Generator(device=device).manual_seed(seed)
+    h = 1.0 / (n + 1)
+    k = torch.arange(1, n + 1, dtype=torch.float64, device=device)
+    kk = torch.sqrt(k[:, None, None] ** 2 + k[None, :, None] ** 2 + k[None, None, :] ** 2)
+    lam1 = (2.0 - 2.0 * torch.cos(math.pi * k / (n + 1))) / (h * h)
+    lam = lam1[:, None, None] + lam1[None, :, None] + lam1[None, None, :]
+    out = torch.empty((nb, n, n, n), dtype=torch.float64, device=device)
+    for b in range(nb):
+        alpha = 1.0 + 2.0 * torch.rand((), generator=g, dtype=torch.float64,
+                                       device=device).item()
+        coef = torch.randn((n, n, n), generator=g, dtype=torch.float64,
+                           device=device) * kk ** (-alpha)
+        t = (coef * lam)[None]
+        for d in (1, 2, 3):
+            t = _dst1(t, d)
+        t = t[0]
+        out[b] = t / t.pow(2).mean().sqrt()
+    return out

@@ -1,12 +1,18 @@
 """Trains the Poisson warm-start network (ssam_cnn_*) on the GPU.
 
 Training set: 4096 pairs (f, u) at n^3 = 128^3 -- f = gaussian_rhs_torch(8,
-n, seed) for 512 seeds (8 right-hand sides each), u = A^-1 f, the exact
-discrete solution of the 7-point problem (poisson_dst.solve, a type-I sine
-transform solve, checked here with the FP64 residual kernel).  The pairs are
-regenerated on the device for every batch instead of being stored (64 GB at
-FP32).  Seeds of the training set start at 100000, so the benchmark and test
-right-hand sides (small seeds) are never seen in training.
+n, seed) for 512 seeds (8 right-hand sides each; with --mix m, a fraction m
+of the batches are poisson_dst.random_spectrum_rhs instead, so the network
+also meets the rough and smooth inputs that residuals inside defect
+correction are) and u the plain solver's answer (ssam_poisson_solve: FP32
+Jacobi sweeps inside the FP64 defect correction, to --target-tol relative
+residual, 64 right-hand sides per solve).  The solutions are kept on the
+device in FP32 (8 MiB each); the right-hand sides are regenerated from their
+seeds for every batch.  A sample of the solutions is compared with the exact
+discrete solution (poisson_dst.solve, a type-I sine transform).  With
+--targets exact the sine-transform solutions are used directly.  Seeds of the
+training set start at 100000, so the benchmark and test right-hand sides
+(small seeds) are never seen in training.
 
 Each step is one forward + backward through the library's tcgen05 kernels
 (ssam_cnn_gradient) and one Adam step (ssam_cnn_adam_step); the learning rate
@@ -48,6 +54,10 @@ def main(argv=None):
     ap.add_argument("--out", default="ssam_b200/data/poisson_cnn_n128.bin")
     ap.add_argument("--log", default=None)
     ap.add_argument("--eval-every", type=int, default=64)
+    ap.add_argument("--targets", choices=["solver", "exact"], default="solver")
+    ap.add_argument("--target-tol", type=float, default=1e-4)
+    ap.add_argument("--mix", type=float, default=0.5,
+                    help="fraction of batches with random-spectrum right-hand sides")
     a = ap.parse_args(argv)
 
     dev = torch.device("cuda", 0)
@@ -66,20 +76,59 @@ def main(argv=None):
         logf.flush()
         print(json.dumps(rec), flush=True)
 
+    n_spec = int(round(a.mix * nbatches))
+
+    def rhs(i):
+        """Right-hand sides of training batch i."""
+        if i >= nbatches - n_spec:
+            return poisson_dst.random_spectrum_rhs(a.batch, a.n, TRAIN_SEED0 + 50000 + i, dev)
+        return gaussian_rhs_torch(a.batch, a.n, TRAIN_SEED0 + i, dev)
+
     f_eval = gaussian_rhs_torch(a.batch, a.n, EVAL_SEED, dev)
     u_eval = poisson_dst.solve(f_eval)
-    worst = max(ssam.poisson_residual(f_eval, u_eval))
+    f_spec = poisson_dst.random_spectrum_rhs(a.batch, a.n, EVAL_SEED, dev)
+    u_spec = poisson_dst.solve(f_spec)
+    worst = max(ssam.poisson_residual(f_eval, u_eval) + ssam.poisson_residual(f_spec, u_spec))
     if worst > 1e-10:
-        raise RuntimeError(f"sine-transform targets have residual {worst:.3g}")
+        raise RuntimeError(f"sine-transform solution has residual {worst:.3g}")
+
+    def rel_err(w, u):
+        return ((w - u).flatten(1).norm(dim=1) / u.flatten(1).norm(dim=1)).max().item()
 
     def evaluate():
         w = net.forward(f_eval)
-        rel_res = ssam.poisson_residual(f_eval, w)
-        err = ((w - u_eval).flatten(1).norm(dim=1) / u_eval.flatten(1).norm(dim=1)).tolist()
-        return max(rel_res), max(err)
+        return {"eval_warm_start_residual": max(ssam.poisson_residual(f_eval, w)),
+                "eval_rel_error": rel_err(w, u_eval),
+                "eval_spectrum_rel_error": rel_err(net.forward(f_spec), u_spec)}
 
     log({"event": "start", "n": a.n, "batch": a.batch, "pairs": a.pairs, "steps": steps,
-         "lr": a.lr, "params": net.num_params, "target_residual": worst})
+         "lr": a.lr, "params": net.num_params, "targets": a.targets, "mix": a.mix})
+
+    # the plain solver's answers for every training pair, 64 rhs per solve
+    solved = None
+    if a.targets == "solver":
+        t0 = time.time()
+        solved = torch.empty((nbatches * a.batch, a.n, a.n, a.n), dtype=torch.float32,
+                             device=dev)
+        per = max(1, 64 // a.batch)
+        sweeps = 0
+        dev_rel = None
+        for c0 in range(0, nbatches, per):
+            ids = list(range(c0, min(nbatches, c0 + per)))
+            f = torch.cat([rhs(i) for i in ids])
+            u = torch.zeros_like(f)
+            st = ssam.poisson_solve(f, u, tol=a.target_tol, sweep_dtype="f32",
+                                    sweeps_per_correction=2000, max_sweeps=400000)
+            if not st["converged"]:
+                raise RuntimeError(f"plain solver did not converge: {st}")
+            sweeps += st["sweeps"]
+            solved[c0 * a.batch:(c0 + len(ids)) * a.batch] = u.float()
+            if c0 == 0:
+                exact = poisson_dst.solve(f[:a.batch])
+                dev_rel = rel_err(u[:a.batch], exact)
+            del f, u
+        log({"event": "targets", "solver_sweeps": sweeps, "seconds": time.time() - t0,
+             "tol": a.target_tol, "max_rel_error_vs_exact_first_batch": dev_rel})
     g = torch.Generator().manual_seed(a.seed)
     order = []
     t_start = time.time()
@@ -87,9 +136,12 @@ def main(argv=None):
     for step in range(steps):
         if not order:
             order = torch.randperm(nbatches, generator=g).tolist()
-        seed = TRAIN_SEED0 + order.pop()
-        f = gaussian_rhs_torch(a.batch, a.n, seed, dev)
-        u = poisson_dst.solve(f)
+        idx = order.pop()
+        f = rhs(idx)
+        if solved is not None:
+            u = solved[idx * a.batch:(idx + 1) * a.batch].double()
+        else:
+            u = poisson_dst.solve(f)
         if step < a.warmup:
             lr = a.lr * (step + 1) / a.warmup
         else:
@@ -104,15 +156,12 @@ def main(argv=None):
         if not math.isfinite(loss):
             raise RuntimeError(f"loss is {loss} at step {step}")
         if step % a.eval_every == 0 or step == steps - 1:
-            res, err = evaluate()
-            log({"step": step, "loss": loss, "lr": lr, "eval_warm_start_residual": res,
-                 "eval_rel_error": err, "ms_per_step": 1e3 * t_steps / (step + 1),
-                 "elapsed_s": time.time() - t_start})
+            log({"step": step, "loss": loss, "lr": lr, **evaluate(),
+                 "ms_per_step": 1e3 * t_steps / (step + 1), "elapsed_s": time.time() - t_start})
     net.save(a.out)
-    res, err = evaluate()
-    log({"event": "done", "steps": steps, "eval_warm_start_residual": res,
-         "eval_rel_error": err, "ms_per_step": 1e3 * t_steps / max(1, steps),
-         "elapsed_s": time.time() - t_start, "weights": os.path.basename(a.out)})
+    log({"event": "done", "steps": steps, **evaluate(),
+         "ms_per_step": 1e3 * t_steps / max(1, steps), "elapsed_s": time.time() - t_start,
+         "weights": os.path.basename(a.out)})
     logf.close()
 
 

@@ -46,6 +46,56 @@ def test_conv3d_forward_vs_torch_cpu(cuda, nsrc, n, dil):
 
 
 @pytest.mark.parametrize("nsrc", [1, 2])
+@pytest.mark.parametrize("n,dil", [(128, 1), (64, 2), (32, 8), (8, 8)])
+def test_conv3d_forward_planes_at_network_sizes(cuda, nsrc, n, dil):
+    """The level sizes and dilations the network runs (n = 128 at the top,
+    dilation 8 at the bottom, dilations >= n where every off-centre tap is
+    outside the grid), checked on a few output planes."""
+    g = torch.Generator().manual_seed(n + 100 * dil + nsrc)
+    xs = [torch.randn(1, n, n, n, 16, generator=g).to(torch.bfloat16) for _ in range(nsrc)]
+    w = (torch.randn(16, 27, 16 * nsrc, generator=g) * 0.1).to(torch.bfloat16)
+    out = S.cnn_conv3d(xs[0].to(cuda), w.to(cuda), xs[1].to(cuda) if nsrc == 2 else None,
+                       dilation=dil, scale=1.0).double().cpu()
+    x = torch.cat([a.double() for a in xs], dim=-1).permute(0, 4, 1, 2, 3)
+    xp = F.pad(x, (dil,) * 6)
+    wt = to_torch_weight(w)
+    for z in sorted({0, 1, n // 2, n - 1}):
+        want = F.conv3d(xp[:, :, z:z + 2 * dil + 1], wt, dilation=dil)[0, :, 0].permute(1, 2, 0)
+        mag = F.conv3d(xp[:, :, z:z + 2 * dil + 1].abs(), wt.abs(),
+                       dilation=dil)[0, :, 0].permute(1, 2, 0)
+        err = (out[0, z] - want).abs() - (2.0**-8 * want.abs() + 1e-5 * mag)
+        assert err.max().item() <= 0, f"plane {z}: max excess {err.max().item()}"
+
+
+def test_conv3d_gather_kernel_vs_torch_cpu(cuda):
+    """The register-gather kernel (used where the TMA kernel's plan does not
+    fit) on the same check, forced by SSAM_CONV_GATHER=1 in a child process."""
+    import os
+    import subprocess
+    import sys
+    code = (
+        "import torch, torch.nn.functional as F, ssam_b200 as S\n"
+        "g = torch.Generator().manual_seed(5)\n"
+        "x = torch.randn(2, 16, 16, 16, 16, generator=g).to(torch.bfloat16)\n"
+        "w = (torch.randn(16, 27, 16, generator=g) * 0.1).to(torch.bfloat16)\n"
+        "out = S.cnn_conv3d(x.cuda(), w.cuda(), None, dilation=2, scale=1.0).double().cpu()\n"
+        "wt = torch.zeros(16, 16, 3, 3, 3, dtype=torch.float64)\n"
+        "for t in range(27): wt[:, :, t // 9, (t // 3) % 3, t % 3] = w[:, t, :].double()\n"
+        "want = F.conv3d(x.double().permute(0, 4, 1, 2, 3), wt, padding=2, dilation=2)"
+        ".permute(0, 2, 3, 4, 1)\n"
+        "mag = F.conv3d(x.double().abs().permute(0, 4, 1, 2, 3), wt.abs(), padding=2,"
+        " dilation=2).permute(0, 2, 3, 4, 1)\n"
+        "err = (out - want).abs() - (2.0**-8 * want.abs() + 1e-5 * mag)\n"
+        "assert err.max().item() <= 0, err.max().item()\n"
+        "print('ok')\n")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, SSAM_CONV_GATHER="1", PYTHONPATH=root)
+    r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr
+
+
+@pytest.mark.parametrize("nsrc", [1, 2])
 @pytest.mark.parametrize("n,dil", [(16, 1), (32, 1), (32, 2)])
 def test_conv3d_weight_grad_vs_torch_autograd(cuda, nsrc, n, dil):
     g = torch.Generator().manual_seed(n + dil * 7 + nsrc)

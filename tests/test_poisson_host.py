@@ -30,3 +30,13 @@ def test_sine_transform_solve_matches_converged_jacobi():
     u = poisson_dst.solve(torch.from_numpy(f)).numpy()
     uj = oracle.jacobi7(f, np.zeros_like(f), 3000)
     np.testing.assert_allclose(uj, u, rtol=0, atol=1e-10 * np.abs(u).max())
+
+
+def test_random_spectrum_rhs_is_unit_rms_and_seeded():
+    a = poisson_dst.random_spectrum_rhs(2, 12, 4, "cpu")
+    b = poisson_dst.random_spectrum_rhs(2, 12, 4, "cpu")
+    assert torch.equal(a, b)
+    np.testing.assert_allclose(a.pow(2).mean(dim=(1, 2, 3)).numpy(), 1.0, rtol=1e-12)
+    u = poisson_dst.solve(a).numpy()
+    _, rel = oracle.residual7(a.numpy(), u)
+    assert rel.max() < 1e-12
