@@ -194,6 +194,19 @@ conv3d_tma_kernel(const __grid_constant__ CUtensorMap m00, const __grid_constant
   } else if (warp == 1) {
     // ---------------------------------------------------------- MMA issuer
     if (lane == 0) {
+      // descriptors are formed once: a tap's A operand is the stage's base
+      // descriptor plus a constant offset (16-byte units in the address
+      // field, which stays below 2^14 for every shared-memory address)
+      int toff[27];
+#pragma unroll
+      for (int tap = 0; tap < 27; ++tap) {
+        const int dz = tap / 9, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+        toff[tap] = dz * (a.slab_stride >> 4) + dil * xp + (dy * xp + dx) * dil;
+      }
+      const uint64_t abase0 = tc::smem_desc(St + kFrontGuard * 16,
+                                            (uint32_t)(3 * a.slab_stride), 128);
+      const uint64_t abase1 = abase0 + (uint64_t)(stage_bytes >> 4);
+      const uint64_t wbase = tc::smem_desc(Ws, 128, 256);
       uint32_t u = 0, items_done = 0;
       bool issued = false;
       for (int64_t it = blockIdx.x; ok && it < a.items; it += gridDim.x, ++items_done) {
@@ -211,18 +224,14 @@ conv3d_tma_kernel(const __grid_constant__ CUtensorMap m00, const __grid_constant
             break;
           }
           tc::tc_fence_after();
-          const unsigned char* stage = St + s * stage_bytes + kFrontGuard * 16;
           for (int t = 0; t < a.tiles; ++t) {
             const uint32_t d = tmem + (uint32_t)(ab * 128 + t * 16);
-#pragma unroll 1
-            for (int tap = 0; tap < 27; ++tap) {
-              const int dz = tap / 9, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-              const int pos = dil * xp + 128 * t + (dy * xp + dx) * dil;
-              const uint64_t da = tc::smem_desc(stage + dz * a.slab_stride + pos * 16,
-                                                (uint32_t)(3 * a.slab_stride), 128);
-              const uint64_t db = tc::smem_desc(Ws + (tap * NSRC + src) * 512, 128, 256);
-              tc::mma_bf16(d, da, db, IDESC, src > 0 || tap > 0);
-            }
+            const uint64_t at = (s ? abase1 : abase0) + (uint64_t)(128 * t);
+#pragma unroll
+            for (int tap = 0; tap < 27; ++tap)
+              tc::mma_bf16(d, at + (uint64_t)toff[tap],
+                           wbase + (uint64_t)((tap * NSRC + src) * 32), IDESC,
+                           src > 0 || tap > 0);
           }
           tc::mma_commit(&empty[s]);
           issued = true;
