@@ -368,17 +368,19 @@ SSAM_API int ssam_poisson_jacobi(const void* rhs, const void* u_in, void* u_out,
 
 /*
  * Tensor-core (tcgen05) building blocks of the Poisson warm-start network.
- * No counterpart in the reference.  Activations are BF16 channels-last
- * (nbatch, n, n, n, 16), n a power of two with n^3 a multiple of 128; a layer
- * reads one or two 16-channel sources (in1 may be NULL).  Weights are BF16
- * (16 out, 27 taps, 16 * nsrc in); tap = (kz*3 + ky)*3 + kx reads offset
- * ((kz-1), (ky-1), (kx-1)) * dilation, zero outside the grid.
+ * No counterpart in the reference.  Activations are BF16 with 16 channels in
+ * "planar halves": (2, nbatch, n, n, n, 8) -- channels 0-7 of every voxel,
+ * then channels 8-15 -- n a power of two (n^3 a multiple of 128); a layer
+ * reads one or two 16-channel sources (in1 may be NULL; out may not alias
+ * in0 or in1).  Weights are BF16 (16 out, 27 taps, 16 * nsrc in); tap =
+ * (kz*3 + ky)*3 + kx reads offset ((kz-1), (ky-1), (kx-1)) * dilation, zero
+ * outside the grid.
  */
 SSAM_API int ssam_cnn_conv3d(const void* in0, const void* in1, const void* weight, void* out,
                              int nbatch, int n, int dilation, float out_scale, void* stream);
 
 /* fp32 weight gradient (16, 27, 16 * nsrc) of ssam_cnn_conv3d for grad_out
- * (BF16 channels-last, 16 channels). */
+ * (BF16, 16 channels, planar halves). */
 SSAM_API int ssam_cnn_conv3d_wgrad(const void* in0, const void* in1, const void* grad_out,
                                    float* dweight, int nbatch, int n, int dilation,
                                    void* stream);

@@ -398,19 +398,31 @@ def star_coeffs_from_matrix(m) -> list[float]:
     return out
 
 
-def cnn_conv3d(x0, weight, x1=None, dilation: int = 1, scale: float = 1.0, out=None,
-               stream=None):
+def to_planar(x):
+    """Channels-last (nb, n, n, n, 16) -> the library's planar halves
+    (2, nb, n, n, n, 8), contiguous."""
+    return x.reshape(*x.shape[:-1], 2, 8).movedim(-2, 0).contiguous()
+
+
+def from_planar(p):
+    """Planar halves (2, nb, n, n, n, 8) -> channels-last (nb, n, n, n, 16)."""
+    return p.movedim(0, -2).reshape(*p.shape[1:-1], 16)
+
+
+def cnn_conv3d(x0, weight, x1=None, dilation: int = 1, scale: float = 1.0, stream=None):
     """3x3x3 convolution of channels-last BF16 activations (nb, n, n, n, 16)
     (x1: optional second 16-channel source) with weights (16, 27, 16 * nsrc)
-    on the tensor cores (``ssam_cnn_conv3d``)."""
+    on the tensor cores (``ssam_cnn_conv3d``, which works on planar halves;
+    the layouts are converted here)."""
     import torch
     nb, n = x0.shape[0], x0.shape[1]
-    if out is None:
-        out = torch.empty_like(x0)
-    _check(lib().ssam_cnn_conv3d(x0.data_ptr(), x1.data_ptr() if x1 is not None else None,
+    p0 = to_planar(x0)
+    p1 = to_planar(x1) if x1 is not None else None
+    out = torch.empty_like(p0)
+    _check(lib().ssam_cnn_conv3d(p0.data_ptr(), p1.data_ptr() if p1 is not None else None,
                                  weight.data_ptr(), out.data_ptr(), nb, n, dilation, scale,
                                  _stream_ptr(x0, stream)))
-    return out
+    return from_planar(out)
 
 
 def cnn_conv3d_wgrad(x0, grad_out, x1=None, dilation: int = 1, stream=None):
@@ -420,8 +432,10 @@ def cnn_conv3d_wgrad(x0, grad_out, x1=None, dilation: int = 1, stream=None):
     nb, n = x0.shape[0], x0.shape[1]
     nsrc = 2 if x1 is not None else 1
     dw = torch.empty(16, 27, 16 * nsrc, dtype=torch.float32, device=x0.device)
-    _check(lib().ssam_cnn_conv3d_wgrad(x0.data_ptr(), x1.data_ptr() if x1 is not None else None,
-                                       grad_out.data_ptr(), dw.data_ptr(), nb, n, dilation,
+    p0, g = to_planar(x0), to_planar(grad_out)
+    p1 = to_planar(x1) if x1 is not None else None
+    _check(lib().ssam_cnn_conv3d_wgrad(p0.data_ptr(), p1.data_ptr() if p1 is not None else None,
+                                       g.data_ptr(), dw.data_ptr(), nb, n, dilation,
                                        _stream_ptr(x0, stream)))
     return dw
 

@@ -30,7 +30,7 @@ NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
 
 # Hand-written (non-generated) translation units.
 SOURCES = ["api.cu", "autotune.cu", "stencil3d.cu", "noalloc.cu", "batched.cu",
-           "poisson.cu", "cnn.cu", "cnn_conv_tma.cu", "cnn_net.cu"]
+           "poisson.cu", "cnn.cu", "cnn_conv_ring.cu", "cnn_net.cu"]
 
 DTYPES = {"f32": "float", "f64": "double", "bf16": "__nv_bfloat16", "f16": "__half"}
 

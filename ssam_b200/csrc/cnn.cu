@@ -1,19 +1,23 @@
 // Warm-start CNN for the Poisson solver: hand-written implicit-GEMM 3D
 // convolutions on the sm_100a tensor cores (tcgen05.mma, TMEM accumulators).
 //
-// Activations are BF16, channels-last [b][z][y][x][16]; a layer reads one or
-// two 16-channel sources (the second is the skip connection of a U-Net
-// decoder, so concatenation is never materialised).  Weights are BF16
-// [co = 16][tap = 27][ci = 16 * nsrc]; tap = (kz*3 + ky)*3 + kx reads the
-// input at offset ((kz-1), (ky-1), (kx-1)) * dilation, zero outside the grid.
+// Activations are BF16 in "planar halves": [2][b][z][y][x][8], channels 0-7
+// of every voxel, then channels 8-15 (half = b * n^3 * 8 elements apart); a
+// layer reads one or two 16-channel sources (the second is the skip
+// connection of a U-Net decoder, so concatenation is never materialised).
+// Weights are BF16 [co = 16][tap = 27][ci = 16 * nsrc]; tap = (kz*3 + ky)*3
+// + kx reads the input at offset ((kz-1), (ky-1), (kx-1)) * dilation, zero
+// outside the grid.
 //
-// Forward (and data-gradient, with mirrored / transposed weights) as a GEMM:
-//   D[voxel, co] = sum_k A[voxel, k] * B[co, k],  k = (tap, ci), both K-major
-// One CTA computes 128 voxels x 16 channels: every K step (one tap x 16
-// channels) the 4 warps gather the 128 neighbour vectors (32 bytes each) into
-// a shared-memory stage, one thread issues a 128x16x16 tcgen05.mma into TMEM,
-// and a tcgen05.commit on the stage's mbarrier frees it for reuse four steps
-// later.  The epilogue reads the accumulators with tcgen05.ld and stores BF16.
+// The forward (and data-gradient, with mirrored / transposed weights)
+// normally runs on the ring kernel of cnn_conv_ring.cu.  The gather kernel
+// here is its cross-check (SSAM_CONV_GATHER=1) as a GEMM
+//   D[voxel, co] = sum_k A[voxel, k] * B[co, k],  k = (tap, ci), both K-major:
+// one CTA computes 128 voxels x 16 channels; every K step (one tap x 16
+// channels) the 4 warps gather the 128 neighbour vectors into a shared-memory
+// stage, one thread issues a 128x16x16 tcgen05.mma into TMEM, and a
+// tcgen05.commit on the stage's mbarrier frees it for reuse four steps later.
+// The epilogue reads the accumulators with tcgen05.ld and stores BF16.
 #include <stdlib.h>
 
 #include <algorithm>
@@ -42,7 +46,8 @@ template <int NSRC>
 __global__ void __launch_bounds__(128)
 conv3d_fwd_kernel(const __nv_bfloat16* __restrict__ in0, const __nv_bfloat16* __restrict__ in1,
                   const __nv_bfloat16* __restrict__ w, __nv_bfloat16* __restrict__ out,
-                  int log2n, int dil, float out_scale, int* err, unsigned long long wait_ns) {
+                  int log2n, int dil, float out_scale, int64_t half, int* err,
+                  unsigned long long wait_ns) {
   constexpr int NK = 27 * NSRC;
   constexpr uint32_t IDESC = tc::idesc_bf16(kTile, 16, 0, 0);
   extern __shared__ unsigned char smem_raw[];
@@ -87,9 +92,9 @@ conv3d_fwd_kernel(const __nv_bfloat16* __restrict__ in0, const __nv_bfloat16* __
     uint4 lo = make_uint4(0, 0, 0, 0), hi = lo;
     if ((unsigned)zz < (unsigned)n && (unsigned)yy < (unsigned)n && (unsigned)xx < (unsigned)n) {
       const __nv_bfloat16* p =
-          (src == 0 ? in0 : in1) + (bofs + ((int64_t)zz << (2 * log2n)) + (yy << log2n) + xx) * 16;
+          (src == 0 ? in0 : in1) + (bofs + ((int64_t)zz << (2 * log2n)) + (yy << log2n) + xx) * 8;
       lo = __ldg(reinterpret_cast<const uint4*>(p));
-      hi = __ldg(reinterpret_cast<const uint4*>(p) + 1);
+      hi = __ldg(reinterpret_cast<const uint4*>(p + half));
     }
     unsigned char* a = arow + stage * kAStageBytes;
     *reinterpret_cast<uint4*>(a) = lo;
@@ -113,9 +118,8 @@ conv3d_fwd_kernel(const __nv_bfloat16* __restrict__ in0, const __nv_bfloat16* __
   __nv_bfloat16* ob = reinterpret_cast<__nv_bfloat16*>(o);
 #pragma unroll
   for (int i = 0; i < 16; ++i) ob[i] = __float2bfloat16_rn(acc[i] * out_scale);
-  uint4* dst = reinterpret_cast<uint4*>(out + v * 16);
-  dst[0] = o[0];
-  dst[1] = o[1];
+  *reinterpret_cast<uint4*>(out + v * 8) = o[0];
+  *reinterpret_cast<uint4*>(out + half + v * 8) = o[1];
   tc::tc_fence_before();
   __syncthreads();
   tc::tc_fence_after();
@@ -200,7 +204,7 @@ conv3d_wgrad_kernel(const __nv_bfloat16* __restrict__ x0, const __nv_bfloat16* _
           // NSRC sources: channel chunk c of source `src` -- handled by the caller
           // launching one M-tile set per source (x1 unused when NSRC == 1)
           const __nv_bfloat16* src = x0;
-          val = __ldg(reinterpret_cast<const uint4*>(src + nb * 16) + c);
+          val = __ldg(reinterpret_cast<const uint4*>(src + c * nvox * 8 + nb * 8));
         }
       }
       // m = tl*16 + c*8 .. +7 -> MN group tl*2 + c; K row k
@@ -211,7 +215,7 @@ conv3d_wgrad_kernel(const __nv_bfloat16* __restrict__ x0, const __nv_bfloat16* _
       const int c = p & 1, k = (p >> 1) & 15, st = p >> 5;
       const int64_t v = vs + st * kWgStepVox + k;
       uint4 val = make_uint4(0, 0, 0, 0);
-      if (v < v_end) val = __ldg(reinterpret_cast<const uint4*>(g + v * 16) + c);
+      if (v < v_end) val = __ldg(reinterpret_cast<const uint4*>(g + c * nvox * 8 + v * 8));
       unsigned char* b = Bs + (stage * kWgStepsPerStage + st) * kWgBStep;
       *reinterpret_cast<uint4*>(b + c * B_SBO + (k >> 3) * B_LBO + (k & 7) * 16) = val;
     }
@@ -273,13 +277,11 @@ int log2_exact(int n) {
 
 }  // namespace
 
-// out = conv3d(in0 (+ in1 as channels 16..31), w) * out_scale over nb grids of
-// n^3 (n a power of two, n^3 a multiple of 128).
-int conv3d_fwd_tma(const void* in0, const void* in1, const void* w, void* out, int nb, int n,
-                   int dil, float out_scale, cudaStream_t s);
+int conv3d_ring(const void* in, const void* addend, const void* w, int ci_total, int ci_off,
+                void* out, int nb, int n, int dil, float out_scale, cudaStream_t s);
 
 // SSAM_CONV_GATHER=1 in the environment forces the gather kernel (to check
-// it against the same oracle as the TMA kernel).
+// it against the same oracle as the ring kernel).
 static bool force_gather() {
   static const bool v = [] {
     const char* e = getenv("SSAM_CONV_GATHER");
@@ -288,12 +290,21 @@ static bool force_gather() {
   return v;
 }
 
+// out = conv3d(in0 (+ in1 as channels 16..31), w) * out_scale over nb grids
+// of n^3, planar-halves layout.  The ring kernel runs one source per pass; a
+// second source is a second pass that adds the first one's (BF16) result.
 int conv3d_fwd(const void* in0, const void* in1, const void* w, void* out, int nb, int n,
                int dil, float out_scale, cudaStream_t s) {
   if (in0 && w && out &&
       ((uintptr_t)in0 | (uintptr_t)w | (uintptr_t)out | (uintptr_t)in1) % 16 == 0 &&
       !force_gather()) {
-    const int st = conv3d_fwd_tma(in0, in1, w, out, nb, n, dil, out_scale, s);
+    int st;
+    if (in1) {
+      st = conv3d_ring(in1, nullptr, w, 32, 16, out, nb, n, dil, out_scale, s);
+      if (st == SSAM_OK) st = conv3d_ring(in0, out, w, 32, 0, out, nb, n, dil, out_scale, s);
+    } else {
+      st = conv3d_ring(in0, nullptr, w, 16, 0, out, nb, n, dil, out_scale, s);
+    }
     if (st != SSAM_ERR_UNSUPPORTED) return st;
   }
   const int l2 = log2_exact(n);
@@ -306,6 +317,7 @@ int conv3d_fwd(const void* in0, const void* in1, const void* w, void* out, int n
   int st = device_error_word(&err);
   if (st != SSAM_OK) return st;
   const int64_t tiles = (int64_t)nb * n * n * n / kTile;
+  const int64_t half = (int64_t)nb * n * n * n * 8;
   const unsigned long long ns = 1000ull * 1000ull * 1000ull;
   if (in1) {
     constexpr int SM = conv_smem_bytes<2>();
@@ -317,12 +329,12 @@ int conv3d_fwd(const void* in0, const void* in1, const void* w, void* out, int n
     }
     conv3d_fwd_kernel<2><<<(unsigned)tiles, 128, SM, s>>>(
         (const __nv_bfloat16*)in0, (const __nv_bfloat16*)in1, (const __nv_bfloat16*)w,
-        (__nv_bfloat16*)out, l2, dil, out_scale, err, ns);
+        (__nv_bfloat16*)out, l2, dil, out_scale, half, err, ns);
   } else {
     constexpr int SM = conv_smem_bytes<1>();
     conv3d_fwd_kernel<1><<<(unsigned)tiles, 128, SM, s>>>(
         (const __nv_bfloat16*)in0, nullptr, (const __nv_bfloat16*)w, (__nv_bfloat16*)out, l2,
-        dil, out_scale, err, ns);
+        dil, out_scale, half, err, ns);
   }
   count_launch();
   SSAM_CUDA_TRY(cudaGetLastError());
@@ -393,5 +405,7 @@ extern "C" int ssam_cnn_conv3d_wgrad(const void* in0, const void* in1, const voi
 extern "C" int ssam_cnn_conv3d(const void* in0, const void* in1, const void* weight, void* out,
                                int nbatch, int n, int dilation, float out_scale, void* stream) {
   if (nbatch < 1 || dilation < 1) return fail(SSAM_ERR_INVALID, "conv3d: bad nbatch / dilation");
+  if (out && (out == in0 || out == in1))
+    return fail(SSAM_ERR_INVALID, "conv3d: out must not alias an input");
   return conv3d_fwd(in0, in1, weight, out, nbatch, n, dilation, out_scale, (cudaStream_t)stream);
 }

@@ -1,0 +1,406 @@
+// Persistent, bulk-copy-fed implicit-GEMM 3D convolution for the warm-start
+// CNN (forward, and the data gradient with mirrored / transposed weights).
+//
+// Activations are "planar halves": [2][nb][n][n][n][8] BF16 -- channels 0-7
+// of every voxel in one plane, channels 8-15 in the next -- so a grid row of
+// one half is n * 16 contiguous bytes and moves as one cp.async.bulk copy.
+//
+// Shared-memory operand trick: the 27 taps of a 3x3x3 convolution read the
+// same input shifted by (dz, dy, dx) * d (d = dilation).  Each input plane a
+// work item needs is staged as a "slab" per half: TY + 2d rows of XP = n + d
+// voxels, row r at voxel r * XP + d (the d voxels before it stay zero).  In
+// that padded, row-major layout a shift by (dy, dx) is a constant offset of
+// (dy * XP + dx) * d voxels, and the zeros between rows are the x-halo of
+// both neighbouring rows.  So the A operand of every tap is a slab seen from
+// another start address: a K-major, no-swizzle UMMA descriptor whose 8-row
+// core matrices are 8 consecutive voxels (SBO = 128 B) and whose two K halves
+// (channels 0-7 / 8-15) are the two half-slabs (LBO).  Rows outside the grid
+// are copied from a row of zeros, so every copy has the same size.
+//
+// A work item is (grid b, TY output rows from y0, a chunk of output planes
+// z0 ..).  With d = 1 it marches in z: planes z0-1 .. z0+ZC are staged once
+// each into a ring of plane slots and every output plane uses three
+// consecutive slots; with d > 1 each output plane stages its own three
+// planes z-d, z, z+d.  Output positions are enumerated in the padded layout,
+// 128 per MMA tile; positions in the gaps or past the last row are computed
+// and discarded.
+//
+// Warp roles (one CTA per SM, persistent over items):
+//   warp 0      producer: 2 * (TY + 2d) row copies per plane into the ring
+//               (mbarrier full / empty per slot)
+//   warp 1      MMA issuer: TILES x 27 tcgen05.mma (128 x 16 x 16, BF16 in,
+//               FP32 in TMEM) per output plane; two accumulator buffers
+//   warps 2-5   epilogue: tcgen05.ld of each tile's accumulators, scale,
+//               add the optional addend, round to BF16, store valid voxels
+// Every wait is bounded by %globaltimer; on expiry the kernel records error
+// code 8 and winds down (drains its copies and MMAs, frees tensor memory).
+#include <string.h>
+
+#include <algorithm>
+
+#include "cnn_tc.cuh"
+
+namespace ssam {
+
+int device_error_word(int** out);
+
+namespace {
+
+constexpr int kFrontGuard = 8;   // voxels (16 B each) before every slab
+constexpr int kMaxTiles = 16;    // 2 accumulator buffers x 16 tiles x 16 columns
+constexpr int kMaxSlots = 8;
+constexpr int kThreads = 192;
+constexpr int kSmemLimit = 227 * 1024;
+constexpr int kMaxRow = 1024;    // voxels per grid row (the zero row's length)
+
+__device__ __align__(16) uint4 g_zero_row[kMaxRow];  // zero-initialised, never written
+
+struct ConvArgs {
+  const __nv_bfloat16* in;      // planar halves
+  const __nv_bfloat16* addend;  // NULL or planar halves, added after scaling
+  const __nv_bfloat16* w;       // [16][27][ci_total]
+  __nv_bfloat16* out;           // planar halves
+  float out_scale;
+  int ci_total, ci_off;         // this pass uses input channels ci_off .. +15
+  int n, dil, ty, xp, tiles, nyb, nzc, zc, box_rows, slab, slots;
+  int64_t half;                 // elements per half-plane: nb * n^3 * 8
+  int64_t items;
+  int* err;
+  unsigned long long wait_ns;
+};
+
+struct Plan {
+  int ty, xp, tiles, box_rows, slab, slots, smem;
+};
+
+// Largest TY (rows per item) with at most kMaxTiles MMA tiles per output
+// plane and a ring of at least 4 plane slots in shared memory.
+bool make_plan(int n, int dil, Plan* p) {
+  const int xp = n + dil;
+  if (n > kMaxRow) return false;
+  for (int ty = std::min(n, 16); ty >= 1; ty /= 2) {
+    const int box_rows = ty + 2 * dil;
+    const int tiles = (ty * xp + 127) / 128;
+    if (tiles > kMaxTiles) continue;
+    const int tail = tiles * 128 - ty * xp + dil;  // reach past the last row of the last tile
+    const int slab = ((kFrontGuard + box_rows * xp + tail) * 16 + 127) / 128 * 128;
+    const int avail = kSmemLimit - 1024 - 27 * 512 - 256;
+    const int slots = std::min(kMaxSlots, avail / (2 * slab));
+    if (slots < 4) continue;
+    // (at least 120 KB, so that one CTA -- and its 512 TMEM columns -- is
+    // alone on its SM)
+    const int smem = std::max(1024 + 27 * 512 + slots * 2 * slab + 256, 120 * 1024);
+    *p = Plan{ty, xp, tiles, box_rows, slab, slots, smem};
+    return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_addr(b)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_addr(b)) : "memory");
+}
+// Contiguous global -> shared copy (16-byte aligned, size a multiple of 16),
+// completion counted on `bar`.  No multicast.
+__device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_t bytes,
+                                          uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(dst),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+
+struct Item {
+  int b, y0, z0, nout, len;  // len: plane positions the item streams
+};
+
+__device__ __forceinline__ Item decode(const ConvArgs& a, int64_t it) {
+  Item m;
+  m.y0 = (int)(it % a.nyb) * a.ty;
+  const int64_t r = it / a.nyb;
+  const int zci = (int)(r % a.nzc);
+  m.b = (int)(r / a.nzc);
+  m.z0 = zci * a.zc;
+  m.nout = min(a.zc, a.n - m.z0);
+  m.len = a.dil == 1 ? m.nout + 2 : 3 * m.nout;
+  return m;
+}
+
+// The grid plane staged at stream position p of an item.
+__device__ __forceinline__ int plane_at(const ConvArgs& a, const Item& m, int p) {
+  return a.dil == 1 ? m.z0 - 1 + p : m.z0 + p / 3 + (p % 3 - 1) * a.dil;
+}
+
+__global__ void __launch_bounds__(kThreads, 1) conv3d_ring_kernel(ConvArgs a) {
+  constexpr uint32_t IDESC = tc::idesc_bf16(128, 16, 0, 0);
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  unsigned char* Ws = base;
+  unsigned char* Ring = Ws + 27 * 512;
+  const int slot_bytes = 2 * a.slab;
+  const int S = a.slots;
+  uint64_t* full = (uint64_t*)(Ring + S * slot_bytes);
+  uint64_t* empty = full + kMaxSlots;
+  uint64_t* accf = empty + kMaxSlots;
+  uint64_t* acce = accf + 2;
+  uint64_t* drain = acce + 2;
+  uint32_t* tmem_slot = (uint32_t*)(drain + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n = a.n, dil = a.dil, xp = a.xp;
+  // weights -> canonical K-major B tiles (one per tap)
+  for (int idx = threadIdx.x; idx < 27 * 32; idx += kThreads) {
+    const int tap = idx >> 5, co = (idx >> 1) & 15, c = idx & 1;
+    const uint4 v = *reinterpret_cast<const uint4*>(
+        a.w + ((size_t)co * 27 + tap) * a.ci_total + a.ci_off + c * 8);
+    *reinterpret_cast<uint4*>(Ws + tap * 512 + (co >> 3) * 256 + c * 128 + (co & 7) * 16) = v;
+  }
+  // zero the ring once: the gaps between rows and the guards are never copied to
+  for (int idx = threadIdx.x; idx < S * slot_bytes / 16; idx += kThreads)
+    reinterpret_cast<uint4*>(Ring)[idx] = make_uint4(0, 0, 0, 0);
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < S; ++i) {
+      tc::mbar_init(&full[i], 1);
+      tc::mbar_init(&empty[i], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      tc::mbar_init(&accf[i], 1);
+      tc::mbar_init(&acce[i], 128);
+    }
+    tc::mbar_init(drain, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) tc::tmem_alloc(tmem_slot, 512);
+  tc::fence_async_smem();
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  bool ok = true;
+  if (warp == 0) {
+    // ---------------------------------------------------------- producer
+    const uint32_t row_bytes = (uint32_t)n * 16;
+    const uint32_t plane_bytes = 2u * a.box_rows * row_bytes;
+    uint32_t gp = 0;  // stream position over all items
+    for (int64_t it = blockIdx.x; ok && it < a.items; it += gridDim.x) {
+      const Item m = decode(a, it);
+      for (int p = 0; p < m.len; ++p, ++gp) {
+        const int s = (int)(gp % S);
+        const uint32_t use = gp / S;
+        int good = 1;
+        if (lane == 0) {
+          if (use > 0 && !tc::mbar_wait(&empty[s], (use - 1) & 1, a.wait_ns)) good = 0;
+          if (good) mbar_expect_tx(&full[s], plane_bytes);
+        }
+        good = __shfl_sync(0xffffffffu, good, 0);
+        if (!good) {
+          ok = false;
+          break;
+        }
+        const int z = plane_at(a, m, p);
+        const uint32_t bar = tc::smem_addr(&full[s]);
+        unsigned char* slot = Ring + s * slot_bytes;
+        for (int k = lane; k < 2 * a.box_rows; k += 32) {
+          const int h = k / a.box_rows, r = k % a.box_rows;
+          const int y = m.y0 - dil + r;
+          const void* src = g_zero_row;
+          if (z >= 0 && z < n && y >= 0 && y < n)
+            src = a.in + h * a.half + ((((int64_t)m.b * n + z) * n + y) * n) * 8;
+          bulk_copy(tc::smem_addr(slot + h * a.slab + (kFrontGuard + r * xp + dil) * 16), src,
+                    row_bytes, bar);
+        }
+        __syncwarp();
+      }
+    }
+    // the last copies must land before the CTA exits
+    if (lane == 0)
+      for (uint32_t k = gp > (uint32_t)S ? gp - S : 0; k < gp; ++k)
+        if (!tc::mbar_wait(&full[k % S], (k / S) & 1, a.wait_ns)) ok = false;
+  } else if (warp == 1) {
+    // ---------------------------------------------------------- MMA issuer
+    if (lane == 0) {
+      // A descriptor of a tap = the slot's base descriptor + a constant
+      // offset (16-byte units; the address field stays below 2^14)
+      int toff[9];
+#pragma unroll
+      for (int t9 = 0; t9 < 9; ++t9) {
+        const int dy = t9 / 3 - 1, dx = t9 % 3 - 1;
+        toff[t9] = kFrontGuard + dil * xp + (dy * xp + dx) * dil;
+      }
+      const uint64_t abase0 = tc::smem_desc(Ring, (uint32_t)a.slab, 128);
+      const uint64_t wbase = tc::smem_desc(Ws, 128, 256);
+      uint32_t gbase = 0, outs = 0;
+      bool issued = false;
+      for (int64_t it = blockIdx.x; ok && it < a.items; it += gridDim.x) {
+        const Item m = decode(a, it);
+        for (int j = 0; j < m.nout; ++j, ++outs) {
+          const int ab = outs & 1;
+          const uint32_t ause = outs >> 1;
+          if (ause > 0 && !tc::mbar_wait(&acce[ab], (ause - 1) & 1, a.wait_ns)) {
+            ok = false;
+            break;
+          }
+          // stream positions of planes z-d, z, z+d
+          const uint32_t q0 = gbase + (dil == 1 ? j : 3 * j);
+          for (int k = 0; k < 3; ++k) {
+            const uint32_t q = q0 + k;
+            if (dil == 1 && j > 0 && k < 2) continue;  // waited for by an earlier plane
+            if (!tc::mbar_wait(&full[q % S], (q / S) & 1, a.wait_ns)) ok = false;
+          }
+          if (!ok) break;
+          tc::tc_fence_after();
+          for (int t = 0; t < a.tiles; ++t) {
+            const uint32_t d = tmem + (uint32_t)(ab * 256 + t * 16);
+#pragma unroll
+            for (int dz = 0; dz < 3; ++dz) {
+              const uint64_t at =
+                  abase0 + (uint64_t)(((q0 + dz) % S) * (slot_bytes >> 4) + 128 * t);
+#pragma unroll
+              for (int t9 = 0; t9 < 9; ++t9)
+                tc::mma_bf16(d, at + (uint64_t)toff[t9], wbase + (uint64_t)((dz * 9 + t9) * 32),
+                             IDESC, dz > 0 || t9 > 0);
+            }
+          }
+          issued = true;
+          tc::mma_commit(&accf[ab]);
+          // release the planes no later output of this item reads
+          if (dil == 1) {
+            tc::mma_commit(&empty[q0 % S]);
+            if (j == m.nout - 1) {
+              tc::mma_commit(&empty[(q0 + 1) % S]);
+              tc::mma_commit(&empty[(q0 + 2) % S]);
+            }
+          } else {
+            for (int k = 0; k < 3; ++k) tc::mma_commit(&empty[(q0 + k) % S]);
+          }
+        }
+        gbase += m.len;
+      }
+      // every MMA issued must finish before tensor memory is released
+      if (issued) {
+        tc::mma_commit(drain);
+        if (!tc::mbar_wait(drain, 0, a.wait_ns)) ok = false;
+      }
+    }
+  } else {
+    // ---------------------------------------------------------- epilogue
+    const int q = warp & 3;  // TMEM lane quarter this warp may read
+    const int row = q * 32 + lane;
+    uint32_t outs = 0;
+    for (int64_t it = blockIdx.x; ok && it < a.items; it += gridDim.x) {
+      const Item m = decode(a, it);
+      for (int j = 0; j < m.nout; ++j, ++outs) {
+        const int ab = outs & 1;
+        if (!tc::mbar_wait(&accf[ab], (outs >> 1) & 1, a.wait_ns)) {
+          ok = false;
+          break;
+        }
+        tc::tc_fence_after();
+        const int64_t zrow = ((int64_t)m.b * n + m.z0 + j) * n;
+        for (int t = 0; t < a.tiles; ++t) {
+          float v[16];
+          tc::tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * 256 + t * 16), v);
+          const int p = 128 * t + row;
+          const int r = p / xp, x = p % xp - dil;
+          if (r < a.ty && x >= 0 && m.y0 + r < n) {
+            const int64_t e = ((zrow + m.y0 + r) * n + x) * 8;
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] *= a.out_scale;
+            if (a.addend) {
+              const uint4 u0 = *reinterpret_cast<const uint4*>(a.addend + e);
+              const uint4 u1 = *reinterpret_cast<const uint4*>(a.addend + a.half + e);
+              const __nv_bfloat16* b0 = reinterpret_cast<const __nv_bfloat16*>(&u0);
+              const __nv_bfloat16* b1 = reinterpret_cast<const __nv_bfloat16*>(&u1);
+#pragma unroll
+              for (int i = 0; i < 8; ++i) {
+                v[i] += __bfloat162float(b0[i]);
+                v[8 + i] += __bfloat162float(b1[i]);
+              }
+            }
+            uint4 o[2];
+            __nv_bfloat16* ob = reinterpret_cast<__nv_bfloat16*>(o);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) ob[i] = __float2bfloat16_rn(v[i]);
+            *reinterpret_cast<uint4*>(a.out + e) = o[0];
+            *reinterpret_cast<uint4*>(a.out + a.half + e) = o[1];
+          }
+        }
+        tc::tc_fence_before();
+        mbar_arrive(&acce[ab]);
+      }
+    }
+  }
+  if (!ok) atomicCAS(a.err, 0, 8);
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  if (warp == 1) tc::tmem_free(tmem, 512);
+}
+
+}  // namespace
+
+// One single-source pass: out = conv(in, w[:, :, ci_off .. ci_off+15]) *
+// scale (+ addend).  SSAM_ERR_UNSUPPORTED when the shape has no plan.
+int conv3d_ring(const void* in, const void* addend, const void* w, int ci_total, int ci_off,
+                void* out, int nb, int n, int dil, float out_scale, cudaStream_t s) {
+  Plan p;
+  if (!make_plan(n, dil, &p)) return SSAM_ERR_UNSUPPORTED;
+  ConvArgs a;
+  a.in = (const __nv_bfloat16*)in;
+  a.addend = (const __nv_bfloat16*)addend;
+  a.w = (const __nv_bfloat16*)w;
+  a.out = (__nv_bfloat16*)out;
+  a.out_scale = out_scale;
+  a.ci_total = ci_total;
+  a.ci_off = ci_off;
+  a.n = n;
+  a.dil = dil;
+  a.ty = p.ty;
+  a.xp = p.xp;
+  a.tiles = p.tiles;
+  a.box_rows = p.box_rows;
+  a.slab = p.slab;
+  a.slots = p.slots;
+  a.nyb = (n + p.ty - 1) / p.ty;
+  a.half = (int64_t)nb * n * n * n * 8;
+  a.wait_ns = 1000ull * 1000ull * 1000ull;
+  int st = device_error_word(&a.err);
+  if (st != SSAM_OK) return st;
+  int dev = 0, sms = 0;
+  SSAM_CUDA_TRY(cudaGetDevice(&dev));
+  SSAM_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  // z chunk: fewest rounds x (planes per item incl. the d = 1 prologue)
+  const int64_t cols = (int64_t)nb * a.nyb;
+  int64_t best = -1;
+  for (int nzc = 1; nzc <= n; nzc *= 2) {
+    const int zc = (n + nzc - 1) / nzc;
+    const int64_t items = cols * nzc;
+    const int64_t rounds = (items + sms - 1) / sms;
+    const int64_t cost = rounds * (dil == 1 ? zc + 2 : 3 * zc);
+    if (best < 0 || cost < best) {
+      best = cost;
+      a.nzc = nzc;
+      a.zc = zc;
+      a.items = items;
+    }
+  }
+  static bool attr_set = false;
+  if (!attr_set) {
+    SSAM_CUDA_TRY(cudaFuncSetAttribute(conv3d_ring_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimit));
+    attr_set = true;
+  }
+  const int64_t grid = std::min<int64_t>(a.items, sms);
+  conv3d_ring_kernel<<<(unsigned)grid, kThreads, p.smem, s>>>(a);
+  count_launch();
+  SSAM_CUDA_TRY(cudaGetLastError());
+  return SSAM_OK;
+}
+
+}  // namespace ssam

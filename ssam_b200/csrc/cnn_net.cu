@@ -81,7 +81,7 @@ __global__ void sumsq_finish_kernel(const double* __restrict__ partial, double* 
   }
 }
 
-// x[b][v][0] = f[b][v] / rms_b, channels 1..15 = 0
+// x[b][v][0] = f[b][v] / rms_b, channels 1..15 = 0 (planar halves)
 __global__ void encode_kernel(const double* __restrict__ f, const double* __restrict__ sumsq,
                               bf16* __restrict__ x, int64_t n3, int nb) {
   const int64_t total = n3 * nb;
@@ -92,14 +92,15 @@ __global__ void encode_kernel(const double* __restrict__ f, const double* __rest
     const float v = rms > 0 ? (float)(f[i] / rms) : 0.f;
     uint4 lo = make_uint4(0, 0, 0, 0), hi = lo;
     reinterpret_cast<bf16*>(&lo)[0] = __float2bfloat16_rn(v);
-    uint4* p = reinterpret_cast<uint4*>(x + i * C);
-    p[0] = lo;
-    p[1] = hi;
+    *reinterpret_cast<uint4*>(x + i * 8) = lo;
+    *reinterpret_cast<uint4*>(x + total * 8 + i * 8) = hi;
   }
 }
 
-__device__ __forceinline__ void load16(const bf16* p, float (&v)[16]) {
-  const uint4 a = reinterpret_cast<const uint4*>(p)[0], b = reinterpret_cast<const uint4*>(p)[1];
+// The 16 channels of voxel i of a planar-halves tensor of `nvox` voxels.
+__device__ __forceinline__ void load16(const bf16* t, int64_t i, int64_t nvox, float (&v)[16]) {
+  const uint4 a = *reinterpret_cast<const uint4*>(t + i * 8);
+  const uint4 b = *reinterpret_cast<const uint4*>(t + nvox * 8 + i * 8);
   const bf16* e = reinterpret_cast<const bf16*>(&a);
   const bf16* f = reinterpret_cast<const bf16*>(&b);
 #pragma unroll
@@ -108,7 +109,7 @@ __device__ __forceinline__ void load16(const bf16* p, float (&v)[16]) {
     v[8 + i] = __bfloat162float(f[i]);
   }
 }
-__device__ __forceinline__ void store16(bf16* p, const float (&v)[16]) {
+__device__ __forceinline__ void store16(bf16* t, int64_t i, int64_t nvox, const float (&v)[16]) {
   uint4 a, b;
   bf16* e = reinterpret_cast<bf16*>(&a);
   bf16* f = reinterpret_cast<bf16*>(&b);
@@ -117,8 +118,8 @@ __device__ __forceinline__ void store16(bf16* p, const float (&v)[16]) {
     e[i] = __float2bfloat16_rn(v[i]);
     f[i] = __float2bfloat16_rn(v[8 + i]);
   }
-  reinterpret_cast<uint4*>(p)[0] = a;
-  reinterpret_cast<uint4*>(p)[1] = b;
+  *reinterpret_cast<uint4*>(t + i * 8) = a;
+  *reinterpret_cast<uint4*>(t + nvox * 8 + i * 8) = b;
 }
 
 // 2x2x2 average pool (n -> n/2), 16 channels
@@ -134,13 +135,13 @@ __global__ void pool_kernel(const bf16* __restrict__ x, bf16* __restrict__ y, in
       const int64_t src = ((b * n + 2 * zo + (d >> 2)) * n + 2 * yo + ((d >> 1) & 1)) * n +
                           2 * xo + (d & 1);
       float v[16];
-      load16(x + src * C, v);
+      load16(x, src, total * 8, v);
 #pragma unroll
       for (int c = 0; c < 16; ++c) acc[c] += v[c];
     }
 #pragma unroll
     for (int c = 0; c < 16; ++c) acc[c] *= 0.125f;
-    store16(y + i * C, acc);
+    store16(y, i, total, acc);
   }
 }
 
@@ -155,11 +156,11 @@ __global__ void pool_back_kernel(const bf16* __restrict__ gy, bf16* __restrict__
     const int64_t b = i / ((int64_t)n * n * n);
     const int64_t p = ((b * h + z / 2) * h + y / 2) * h + x / 2;
     float v[16], o[16];
-    load16(gy + p * C, v);
-    if (add) load16(gx + i * C, o);
+    load16(gy, p, total / 8, v);
+    if (add) load16(gx, i, total, o);
 #pragma unroll
     for (int c = 0; c < 16; ++c) o[c] = (add ? o[c] : 0.f) + 0.125f * v[c];
-    store16(gx + i * C, o);
+    store16(gx, i, total, o);
   }
 }
 
@@ -172,8 +173,10 @@ __global__ void up_kernel(const bf16* __restrict__ x, bf16* __restrict__ y, int 
     const int xo = (int)(i % m), yo = (int)((i / m) % m), zo = (int)((i / m / m) % m);
     const int64_t b = i / ((int64_t)m * m * m);
     const int64_t src = ((b * n + zo / 2) * n + yo / 2) * n + xo / 2;
-    reinterpret_cast<uint4*>(y + i * C)[0] = reinterpret_cast<const uint4*>(x + src * C)[0];
-    reinterpret_cast<uint4*>(y + i * C)[1] = reinterpret_cast<const uint4*>(x + src * C)[1];
+    const int64_t xv = total / 8;  // voxels of the coarse tensor
+    *reinterpret_cast<uint4*>(y + i * 8) = *reinterpret_cast<const uint4*>(x + src * 8);
+    *reinterpret_cast<uint4*>(y + total * 8 + i * 8) =
+        *reinterpret_cast<const uint4*>(x + xv * 8 + src * 8);
   }
 }
 
@@ -191,11 +194,11 @@ __global__ void up_back_kernel(const bf16* __restrict__ gy, bf16* __restrict__ g
       const int64_t src = ((b * m + 2 * z + (d >> 2)) * m + 2 * y + ((d >> 1) & 1)) * m +
                           2 * x + (d & 1);
       float v[16];
-      load16(gy + src * C, v);
+      load16(gy, src, total * 8, v);
 #pragma unroll
       for (int c = 0; c < 16; ++c) acc[c] += v[c];
     }
-    store16(gx + i * C, acc);
+    store16(gx, i, total, acc);
   }
 }
 
@@ -204,11 +207,11 @@ __global__ void add_kernel(bf16* __restrict__ a, const bf16* __restrict__ b, int
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nvox;
        i += (int64_t)gridDim.x * blockDim.x) {
     float u[16], v[16];
-    load16(a + i * C, u);
-    load16(b + i * C, v);
+    load16(a, i, nvox, u);
+    load16(b, i, nvox, v);
 #pragma unroll
     for (int c = 0; c < 16; ++c) u[c] += v[c];
-    store16(a + i * C, u);
+    store16(a, i, nvox, u);
   }
 }
 
@@ -220,7 +223,7 @@ __global__ void head_kernel(const bf16* __restrict__ x, const float* __restrict_
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
        i += (int64_t)gridDim.x * blockDim.x) {
     float v[16];
-    load16(x + i * C, v);
+    load16(x, i, total, v);
     float s = 0.f;
 #pragma unroll
     for (int c = 0; c < 16; ++c) s = fmaf(wh[c], v[c], s);
@@ -244,7 +247,7 @@ __global__ void head_loss_back_kernel(const bf16* __restrict__ x, const float* _
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
        i += (int64_t)gridDim.x * blockDim.x) {
     float v[16];
-    load16(x + i * C, v);
+    load16(x, i, total, v);
     float y = 0.f;
 #pragma unroll
     for (int c = 0; c < 16; ++c) y = fmaf(wh[c], v[c], y);
@@ -260,7 +263,7 @@ __global__ void head_loss_back_kernel(const bf16* __restrict__ x, const float* _
       o[c] = g * wh[c];
       gw[c] = fmaf(g, v[c], gw[c]);
     }
-    store16(gx + i * C, o);
+    store16(gx, i, total, o);
   }
   for (int c = 0; c < 16; ++c) {
     float s = gw[c];
