@@ -157,9 +157,35 @@ def build(jobs: int | None = None, ptxas_verbose: bool = False, quiet: bool = Tr
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     os.replace(tmp, LIB)
+    build_cli()
     if not quiet:
-        print(f"built {LIB} from {len(objs)} units")
+        print(f"built {LIB} from {len(objs)} units, and the ssai-* programs in {BIN}")
     return LIB
+
+
+BIN = os.path.join(HERE, "bin")
+CLI = {"ssai-2dstencil": "ssai_2dstencil.cpp", "ssai-2dconv": "ssai_2dconv.cpp",
+       "ssai-3dstencil": "ssai_3dstencil.cpp"}
+
+
+def build_cli() -> None:
+    """The reference-spelling command-line drop-ins (host C++ over the C ABI),
+    linked against the library with an rpath to it."""
+    os.makedirs(BIN, exist_ok=True)
+    inc = os.path.join(os.path.dirname(HERE), "include")
+    for exe, src in CLI.items():
+        src = os.path.join(HERE, "cli", src)
+        out = os.path.join(BIN, exe)
+        if (os.path.exists(out) and os.path.getmtime(out) >= os.path.getmtime(src)
+                and os.path.getmtime(out) >= os.path.getmtime(LIB)
+                and os.path.getmtime(out) >= os.path.getmtime(os.path.join(HERE, "cli",
+                                                                           "ssai_cli.h"))):
+            continue
+        cmd = [_nvcc(), "-O2", "-std=c++17", "-I", inc, src, "-o", out, "-L", HERE,
+               "-lssam_b200", "-Xlinker", "-rpath,$ORIGIN/.."]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"building {exe} failed:\n{r.stdout}\n{r.stderr}")
 
 
 def main(argv=None) -> None:

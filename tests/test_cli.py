@@ -1,0 +1,58 @@
+"""The reference-spelling command-line drop-ins (ssai-2dstencil, ssai-2dconv,
+ssai-3dstencil): argument handling on the CPU; on a GPU, every stencil name
+runs and passes its own sampled check against a host evaluation."""
+import os
+import subprocess
+
+import pytest
+
+BIN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "ssam_b200",
+                   "bin")
+
+
+def run(exe, *args, timeout=300):
+    return subprocess.run([os.path.join(BIN, exe), *map(str, args)], capture_output=True,
+                          text=True, timeout=timeout)
+
+
+@pytest.mark.parametrize("exe", ["ssai-2dstencil", "ssai-2dconv", "ssai-3dstencil"])
+def test_programs_are_built_and_print_usage(exe):
+    assert os.path.exists(os.path.join(BIN, exe)), "run the build first"
+    r = run(exe)
+    assert r.returncode == 1
+    assert exe in r.stdout
+
+
+def test_unknown_stencil_name_is_refused():
+    r = run("ssai-2dstencil", 64, "7", "float")
+    assert r.returncode == 1 and "do not call" in r.stdout
+    r = run("ssai-3dstencil", "box", "float")
+    assert r.returncode == 1 and "invalid function name" in r.stdout
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("pts", ["5", "9", "13", "17", "21", "25", "64", "81", "121", "tmp_5",
+                                 "tmp_9"])
+@pytest.mark.parametrize("dtype", ["float", "double"])
+def test_2dstencil_names(cuda, pts, dtype):
+    r = run("ssai-2dstencil", 1000, pts, dtype)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "max relative error" in r.stdout
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fsize", [2, 3, 7, 21, 28])
+@pytest.mark.parametrize("dtype", ["float", "double"])
+def test_2dconv_sizes(cuda, fsize, dtype):
+    r = run("ssai-2dconv", dtype, 777, fsize)
+    assert r.returncode == 0, r.stdout + r.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["7pt", "13pt", "poisson"])
+@pytest.mark.parametrize("dtype", ["float", "double"])
+@pytest.mark.parametrize("n,it", [(64, 1), (48, 3)])
+def test_3dstencil_names(cuda, name, dtype, n, it):
+    r = run("ssai-3dstencil", name, dtype, n, it)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "RMS Error" in r.stdout
