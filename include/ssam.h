@@ -400,8 +400,9 @@ SSAM_API int ssam_cnn_set_params(void* handle, const float* host_params);
 /* u0 = network(f): the warm start */
 SSAM_API int ssam_cnn_forward(void* handle, const double* f, double* u0, int nbatch,
                               void* stream);
-/* forward + backward of the mean squared error against `target` (normalised
- * by the input's RMS); `loss` (host) receives it.  Synchronous. */
+/* forward + backward of the loss against `target`: the mean over right-hand
+ * sides of ||u0 - target||^2 / ||target||^2; `loss` (host) receives it.
+ * Synchronous. */
 SSAM_API int ssam_cnn_gradient(void* handle, const double* f, const double* target, int nbatch,
                                double* loss, void* stream);
 /* one Adam step (beta 0.9 / 0.999) with the last gradient */

@@ -232,16 +232,19 @@ __global__ void head_kernel(const bf16* __restrict__ x, const float* __restrict_
   }
 }
 
-// Loss in normalised units: L = mean over voxels of (y - t)^2 with
-// y = sum_c wh[c] x[v][c], t = target / (rms_b * kOutScale).
-// Writes dL/dx (BF16, into gx), accumulates dL/dwh (fp32) and L.
+// Loss: the mean over right-hand sides of the relative squared error
+//   L = (1/nb) sum_b sum_v (y - t)^2 / sum_v t^2,
+// y = sum_c wh[c] x[v][c], t = target / (rms_b * kOutScale) (normalised
+// units), so every right-hand side weighs the same whatever the size of its
+// solution.  tsq[b] = sum_v target^2.  Writes dL/dx (BF16, into gx),
+// accumulates dL/dwh (fp32) and L.
 __global__ void head_loss_back_kernel(const bf16* __restrict__ x, const float* __restrict__ wh,
                                       const double* __restrict__ target,
-                                      const double* __restrict__ sumsq, bf16* __restrict__ gx,
+                                      const double* __restrict__ sumsq,
+                                      const double* __restrict__ tsq, bf16* __restrict__ gx,
                                       float* __restrict__ gwh, double* __restrict__ loss,
                                       int64_t n3, int nb) {
   const int64_t total = n3 * nb;
-  const double inv_n = 1.0 / (double)total;
   float gw[16] = {0};
   double l = 0.0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
@@ -254,9 +257,11 @@ __global__ void head_loss_back_kernel(const bf16* __restrict__ x, const float* _
     const int b = (int)(i / n3);
     const double scale = sqrt(sumsq[b] / (double)n3) * (double)kOutScale;
     const double t = scale > 0 ? target[i] / scale : 0.0;
+    // 1 / (nb * sum_v t^2) in normalised units
+    const double wb = tsq[b] > 0 ? scale * scale / (tsq[b] * (double)nb) : 0.0;
     const double d = (double)y - t;
-    l += d * d;
-    const float g = (float)(2.0 * d * inv_n);
+    l += wb * d * d;
+    const float g = (float)(2.0 * d * wb);
     float o[16];
 #pragma unroll
     for (int c = 0; c < 16; ++c) {
@@ -271,7 +276,7 @@ __global__ void head_loss_back_kernel(const bf16* __restrict__ x, const float* _
     if ((threadIdx.x & 31) == 0) atomicAdd(&gwh[c], s);
   }
   for (int off = 16; off > 0; off >>= 1) l += __shfl_down_sync(0xffffffffu, l, off);
-  if ((threadIdx.x & 31) == 0) atomicAdd(loss, l * inv_n);
+  if ((threadIdx.x & 31) == 0) atomicAdd(loss, l);
 }
 
 // fp32 master [16][27][ci] -> BF16 forward copy, and the data-gradient
@@ -323,7 +328,7 @@ struct Net {
   // activations (BF16, 16 channels) per level, allocated for nb_max
   std::vector<void*> bufs;
   void* wg_work = nullptr;
-  double* scal = nullptr;  // sumsq[nb_max], loss, spare, then kSumBlocks partials per rhs
+  double* scal = nullptr;  // sumsq[nb_max], loss, spare, kSumBlocks partials per rhs, tsq[nb_max]
   bool weights_dirty = true;
 };
 
@@ -452,8 +457,14 @@ int backward(Net& net, const double* target, int nb, cudaStream_t s) {
   const int64_t n3 = (int64_t)n * n * n;
   float* gh = net.g + (net.nparams - 16);
   SSAM_CUDA_TRY(cudaMemsetAsync(gh, 0, 16 * sizeof(float), s));
+  double* part = net.scal + net.nb_max + 2;
+  double* tsq = part + (size_t)kSumBlocks * net.nb_max;
+  sumsq_kernel<<<dim3(kSumBlocks, nb), 256, 0, s>>>(target, n3, part);
+  sumsq_finish_kernel<<<1, 32, 0, s>>>(part, tsq, nb);
+  count_launch();
+  count_launch();
   head_loss_back_kernel<<<grid_for(n3 * nb), 256, 0, s>>>(
-      (const bf16*)net.bufs[D1b], net.w + (net.nparams - 16), target, net.scal,
+      (const bf16*)net.bufs[D1b], net.w + (net.nparams - 16), target, net.scal, tsq,
       (bf16*)net.bufs[GA], gh, net.scal + net.nb_max, n3, nb);
   count_launch();
   // level 1 decoder
@@ -540,7 +551,9 @@ extern "C" int ssam_cnn_create(int n, int nbatch_max, unsigned long long seed, v
   if (e == cudaSuccess) e = cudaMalloc(&net->v, pb);
   if (e == cudaSuccess) e = cudaMalloc(&net->wf, net->nparams * sizeof(bf16));
   if (e == cudaSuccess) e = cudaMalloc(&net->wt, net->nparams * sizeof(bf16));
-  if (e == cudaSuccess) e = cudaMalloc(&net->scal, sizeof(double) * (nbatch_max + 2 + (size_t)kSumBlocks * nbatch_max));
+  if (e == cudaSuccess) e = cudaMalloc(&net->scal,
+                                        sizeof(double) * (2 * (size_t)nbatch_max + 2 +
+                                                          (size_t)kSumBlocks * nbatch_max));
   if (e != cudaSuccess) return bail(e, "cudaMalloc(cnn parameters)");
   e = cudaMemcpy(net->w, w.data(), pb, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemset(net->g, 0, pb);

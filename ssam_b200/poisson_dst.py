@@ -43,26 +43,25 @@ def solve(f):
 
 
 def random_spectrum_rhs(nb: int, n: int, seed: int, device="cuda"):
-    """Right-hand sides whose solutions have random sine-mode spectra with a
-    power-law fall-off |k|^-alpha, alpha ~ U[1, 3] per sample (from rough to
-    smooth solutions); unit RMS.  f = A e for e = DST^-1 of the random
-    coefficients, computed in the spectral domain.  Broadens the training set
-    beyond Gaussian bumps so the network's A^-1 holds across frequency bands
-    (the inputs it meets inside defect correction are residuals, not bumps)."""
+    """Right-hand sides with random sine-mode spectra: coefficient N(0,1) *
+    |k|^-alpha * exp(-|k|^2 / (2 kc^2)) per mode, alpha ~ U[0, 2] and kc
+    log-uniform in [4, 32] per sample, unit RMS.  These are the inputs the
+    network meets inside defect correction: residuals after smoothing sweeps
+    have lost their high-frequency part (the cut-off kc) and carry whatever
+    smooth error the previous correction left (the power law), unlike the
+    localised Gaussian bumps of the benchmark's right-hand sides."""
     import torch
     g = torch.Generator(device=device).manual_seed(seed)
-    h = 1.0 / (n + 1)
     k = torch.arange(1, n + 1, dtype=torch.float64, device=device)
-    kk = torch.sqrt(k[:, None, None] ** 2 + k[None, :, None] ** 2 + k[None, None, :] ** 2)
-    lam1 = (2.0 - 2.0 * torch.cos(math.pi * k / (n + 1))) / (h * h)
-    lam = lam1[:, None, None] + lam1[None, :, None] + lam1[None, None, :]
+    kk2 = k[:, None, None] ** 2 + k[None, :, None] ** 2 + k[None, None, :] ** 2
     out = torch.empty((nb, n, n, n), dtype=torch.float64, device=device)
     for b in range(nb):
-        alpha = 1.0 + 2.0 * torch.rand((), generator=g, dtype=torch.float64,
-                                       device=device).item()
-        coef = torch.randn((n, n, n), generator=g, dtype=torch.float64,
-                           device=device) * kk ** (-alpha)
-        t = (coef * lam)[None]
+        u2 = torch.rand(2, generator=g, dtype=torch.float64, device=device).tolist()
+        alpha = 2.0 * u2[0]
+        kc = 4.0 * 8.0 ** u2[1]
+        coef = torch.randn((n, n, n), generator=g, dtype=torch.float64, device=device)
+        coef = coef * kk2 ** (-alpha / 2) * torch.exp(-kk2 / (2 * kc * kc))
+        t = coef[None]
         for d in (1, 2, 3):
             t = _dst1(t, d)
         t = t[0]

@@ -158,7 +158,9 @@ def mirror_loss(params, f, target=None):
     u0 = y * scale
     loss = None
     if target is not None:
-        loss = ((y - target / scale) ** 2).mean()
+        t = target / scale
+        # mean over right-hand sides of the relative squared error
+        loss = (((y - t) ** 2).sum(dim=(1, 2, 3)) / (t ** 2).sum(dim=(1, 2, 3))).mean()
     return u0, loss
 
 
