@@ -313,6 +313,9 @@ typedef struct ssam_poisson_options {
   int max_sweeps;            /* give up (converged = 0) after this many sweeps */
   double omega;              /* Jacobi damping: u <- (1-w) u + w (nbrs + h^2 r) / 6;
                                 0 is taken as 1 (plain Jacobi) */
+  int cnn_smoothing;         /* learned solve: passes of the 7-point average (centre 1/2,
+                                neighbours 1/12) applied to the network's input and
+                                output; 0 = none */
 } ssam_poisson_options;
 
 typedef struct ssam_poisson_stats {

@@ -48,7 +48,7 @@ class PoissonOptions(ctypes.Structure):
     """``ssam_poisson_options``."""
     _fields_ = [("tol", ctypes.c_double), ("sweep_dtype", ctypes.c_int),
                 ("sweeps_per_correction", ctypes.c_int), ("max_sweeps", ctypes.c_int),
-                ("omega", ctypes.c_double)]
+                ("omega", ctypes.c_double), ("cnn_smoothing", ctypes.c_int)]
 
 
 class PoissonStats(ctypes.Structure):
@@ -309,7 +309,7 @@ def _poisson_grid(t):
 
 def poisson_solve(f, u, tol: float = 1e-5, sweep_dtype=None, sweeps_per_correction: int = 1000,
                   max_sweeps: int = 200000, cnn=None, omega: float = 1.0,
-                  stream=None) -> dict:
+                  cnn_smoothing: int = 4, stream=None) -> dict:
     """``ssam_poisson_solve``: f, u are float64 (nbatch, n, n, n); u holds the
     initial guess and receives the solution.  With ``cnn`` (a WarmStartCNN)
     this is ``ssam_poisson_solve_learned``: the network's correction comes
@@ -319,7 +319,7 @@ def poisson_solve(f, u, tol: float = 1e-5, sweep_dtype=None, sweeps_per_correcti
     if u.shape != f.shape or f.dtype != torch.float64 or u.dtype != torch.float64:
         raise ValueError("f and u must be float64 tensors of the same shape")
     dt = F32 if sweep_dtype in (None, "f32", torch.float32) else BF16
-    opt = PoissonOptions(tol, dt, sweeps_per_correction, max_sweeps, omega)
+    opt = PoissonOptions(tol, dt, sweeps_per_correction, max_sweeps, omega, cnn_smoothing)
     st = PoissonStats()
     if cnn is None:
         _check(lib().ssam_poisson_solve(f.data_ptr(), u.data_ptr(), n, nb, ctypes.byref(opt),

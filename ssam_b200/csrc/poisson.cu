@@ -223,6 +223,26 @@ int cnn_check(void* cnn, int n, int nbatch);
 int cnn_apply(void* cnn, const double* r, double* c, int nbatch, cudaStream_t s);
 }
 
+// `passes` applications of the 7-point average (centre 1/2, neighbours 1/12,
+// zero outside) to buf, ping-ponging with tmp; *out is where the result is.
+// It passes the smooth part of a field and removes its highest frequencies
+// (the sine mode with eigenvalue lambda of -lap is scaled by 1 - lambda h^2/12).
+static int smooth_f64(double* buf, double* tmp, int n, int nb, int passes, const double** out,
+                      cudaStream_t s) {
+  double cube[27] = {0};
+  cube[13] = 0.5;
+  for (int k : {4, 10, 12, 14, 16, 22}) cube[k] = 1.0 / 12.0;
+  double* in = buf;
+  double* o = tmp;
+  for (int i = 0; i < passes; ++i) {
+    const int st = sweep_3d(in, o, n, nb, SSAM_F64, cube, nullptr, 0.0, s);
+    if (st != SSAM_OK) return st;
+    std::swap(in, o);
+  }
+  *out = in;
+  return SSAM_OK;
+}
+
 // Defect-correction solve; with `cnn`, every correction first adds the
 // network's approximate solve of A c = r to u in FP64, then runs the
 // low-precision sweeps on the new residual.  A network cycle is kept when the
@@ -253,7 +273,7 @@ static int poisson_solve(const double* f, double* u, int n, int nbatch,
   const size_t lp_al = (lp + 255) / 256 * 256;
   const size_t f64_al = (cells * sizeof(double) + 255) / 256 * 256;
   void* work = nullptr;
-  int st = scratch_alloc(&work, 3 * lp_al + pbytes + (cnn ? 3 * f64_al : 0), s);
+  int st = scratch_alloc(&work, 3 * lp_al + pbytes + (cnn ? 4 * f64_al : 0), s);
   if (st != SSAM_OK) return st;
   char* w8 = (char*)work;
   void* r_lp = w8;
@@ -266,6 +286,8 @@ static int poisson_solve(const double* f, double* u, int n, int nbatch,
   double* r64 = cnn ? (double*)(w8 + 3 * lp_al + pbytes) : nullptr;
   double* c64 = cnn ? (double*)(w8 + 3 * lp_al + pbytes + f64_al) : nullptr;
   double* u_save = cnn ? (double*)(w8 + 3 * lp_al + pbytes + 2 * f64_al) : nullptr;
+  double* tmp64 = cnn ? (double*)(w8 + 3 * lp_al + pbytes + 3 * f64_al) : nullptr;
+  const int passes = std::max(0, opt->cnn_smoothing);
   std::vector<double> norms2(2 * nbatch);
   bool use_cnn = cnn != nullptr;
   bool first = true;
@@ -340,9 +362,15 @@ static int poisson_solve(const double* f, double* u, int n, int nbatch,
       }
       before_cnn = worst;
       judge_cnn = true;
-      st = cnn_apply(cnn, r64, c64, nbatch, s);
+      // the network sees the smooth part of r, and its BF16 noise is
+      // filtered out of the correction (the sweeps handle the rest)
+      const double* cin = r64;
+      st = smooth_f64(r64, tmp64, n, nbatch, passes, &cin, s);
+      if (st == SSAM_OK) st = cnn_apply(cnn, cin, c64, nbatch, s);
+      const double* cout = c64;
+      if (st == SSAM_OK) st = smooth_f64(c64, tmp64, n, nbatch, passes, &cout, s);
       if (st != SSAM_OK) break;
-      axpy_kernel<<<cblocks, nthreads, 0, s>>>(u, c64, 1.0, (int64_t)cells);
+      axpy_kernel<<<cblocks, nthreads, 0, s>>>(u, cout, 1.0, (int64_t)cells);
       count_launch();
       st = residual(f, u, r_lp, dt, n, nbatch, partials, blocks, d_norms, norms2.data(), s);
       if (st != SSAM_OK) break;
