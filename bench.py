@@ -77,6 +77,9 @@ def workloads():
     for arm in ("plain", "learned"):
         w[f"poisson128x8_{arm}"] = dict(kind="poisson", arm=arm, n=128, nb=8, tol=1e-5,
                                         dtype="f64", r=1, steps=1, boundary="zero")
+    # the warm-start network's forward pass (the learned arm's tensor-core part)
+    w["cnn128x8_forward"] = dict(kind="cnn", n=128, nb=8, dtype="bf16", r=1, steps=1,
+                                 boundary="zero")
     return w
 
 
@@ -344,6 +347,10 @@ def run_reference(args, spec, name):
         return
     if spec["kind"] == "poisson":
         return run_reference_poisson(args, spec, name)
+    if spec["kind"] == "cnn":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no network "
+                          "(the warm start is new work with no reference code)"}), flush=True)
+        return
     n_steps = args.steps + args.warmup
     budget = max(0.05, min(10.0, 150.0 / max(1, n_steps)))
     rates = []
@@ -658,9 +665,7 @@ def run_poisson(args, spec, name):
         b.record(stream)
         torch.cuda.synchronize()
         fwd_ms = a.elapsed_time(b) / 10
-        # 3x3x3 16 -> 16 convolutions: 2 * 27 * 16 * 16 flop per voxel and source
-        units = 5 * n ** 3 + 5 * (n // 2) ** 3 + 4 * (n // 4) ** 3
-        flops = 2 * 27 * 16 * 16 * units * nb
+        flops = cnn_forward_flops(n, nb)
         try:
             with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
                 tpeak, tsrc = float(json.load(fh)["bf16_tflops"]), "measured"
@@ -720,6 +725,87 @@ def run_poisson(args, spec, name):
         net.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def cnn_forward_flops(n, nb):
+    """3x3x3 16 -> 16 convolutions of the network: 2 * 27 * 16 * 16 flop per
+    voxel and source; 5 source-layers at n, 5 at n/2, 4 at n/4."""
+    return 2 * 27 * 16 * 16 * (5 * n ** 3 + 5 * (n // 2) ** 3 + 4 * (n // 4) ** 3) * nb
+
+
+def run_cnn(args, spec, name):
+    """One step = one forward pass of the warm-start network over 8 right-hand
+    sides at 128^3 (input FP64 f, output FP64 u0)."""
+    import torch
+
+    import ssam_b200 as S
+    from ssam_b200.workloads import gaussian_rhs_torch
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n, nb = spec["n"], spec["nb"]
+    f = gaussian_rhs_torch(nb, n, 7 + rank, dev)
+    net = S.WarmStartCNN(n, nb)
+    net.load(CNN_WEIGHTS)
+    out = torch.empty_like(f)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        net.forward(f, out)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    l0 = S.lib().ssam_kernel_launches()
+    a.record(stream)
+    for _ in range(args.steps):
+        net.forward(f, out)
+    b.record(stream)
+    launches = S.lib().ssam_kernel_launches() - l0
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = a.elapsed_time(b) / args.steps
+    flops = cnn_forward_flops(n, nb)
+    value = flops / (ms / 1e3) / 1e12 * world
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            tpeak, tsrc = float(json.load(fh)["bf16_tflops"]), "measured"
+    except Exception:
+        tpeak, tsrc = 1590.0, "fallback"
+    hf = f.cpu().pin_memory()
+    hu = torch.empty_like(hf).pin_memory()
+    k = max(3, min(args.steps, 10))
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(k):
+        f.copy_(hf, non_blocking=True)
+        net.forward(f, out)
+        hu.copy_(out, non_blocking=True)
+    b.record(stream)
+    torch.cuda.synchronize()
+    e_ms = a.elapsed_time(b) / k
+    if rank == 0:
+        print(json.dumps({
+            "metric": "CNN forward TFLOP/s", "value": value, "unit": "TFLOP/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
+            "data": "synthetic (8 Gaussian-bump right-hand sides, seed 7)",
+            "config": {"workload": name, "grid": f"{nb}x{n}^3", "channels": 16,
+                       "weights": os.path.relpath(CNN_WEIGHTS, ROOT),
+                       "l2": "activations 8 x 128^3 x 16 BF16 = 512 MiB per buffer vs 126 MB L2"},
+            "gpu_launches": launches,
+            "roofline": {"bound": "tensor", "achieved": value / world, "peak": tpeak,
+                         "unit": "TFLOP/s", "frac": value / world / tpeak, "peak_source": tsrc,
+                         "traffic": None, "flops_per_forward": flops},
+            "clocks": clk,
+            "e2e": {"value": flops / (e_ms / 1e3) / 1e12, "unit": "TFLOP/s",
+                    "h2d_bytes_per_step": f.numel() * 8, "d2h_bytes_per_step": f.numel() * 8,
+                    "steps": k},
+            "cpu_baseline": None,
+        }), flush=True)
+    net.close()
 
 
 def run_ssam(args, spec, name):
@@ -915,6 +1001,8 @@ def main(argv=None):
         run_batched(args, spec, args.workload)
     elif spec["kind"] == "poisson":
         run_poisson(args, spec, args.workload)
+    elif spec["kind"] == "cnn":
+        run_cnn(args, spec, args.workload)
     else:
         run_ssam(args, spec, args.workload)
 
