@@ -78,8 +78,9 @@ def workloads():
         w[f"poisson128x8_{arm}"] = dict(kind="poisson", arm=arm, n=128, nb=8, tol=1e-5,
                                         dtype="f64", r=1, steps=1, boundary="zero")
     # the warm-start network's forward pass (the learned arm's tensor-core part)
-    w["cnn128x8_forward"] = dict(kind="cnn", n=128, nb=8, dtype="bf16", r=1, steps=1,
-                                 boundary="zero")
+    for nb in (8, 1):  # (the one-grid case is small enough for a full ncu capture)
+        w[f"cnn128x{nb}_forward"] = dict(kind="cnn", n=128, nb=nb, dtype="bf16", r=1, steps=1,
+                                         boundary="zero")
     return w
 
 
