@@ -78,6 +78,10 @@ def workloads():
         w[f"poisson128x8_{arm}"] = dict(kind="poisson", arm=arm, n=128, nb=8, tol=1e-5,
                                         dtype="f64", r=1, steps=1, boundary="zero")
     # the warm-start network's forward pass (the learned arm's tensor-core part)
+    # the Poisson arms' sweep kernel alone: 100 Jacobi sweeps of 8 x 128^3
+    for dt in ("f32", "bf16"):
+        w[f"jacobi128x8_{dt}_100sweeps"] = dict(kind="jacobi", n=128, nb=8, dtype=dt, r=1,
+                                                steps=100, boundary="zero")
     for nb in (8, 1):  # (the one-grid case is small enough for a full ncu capture)
         w[f"cnn128x{nb}_forward"] = dict(kind="cnn", n=128, nb=nb, dtype="bf16", r=1, steps=1,
                                          boundary="zero")
@@ -348,6 +352,11 @@ def run_reference(args, spec, name):
         return
     if spec["kind"] == "poisson":
         return run_reference_poisson(args, spec, name)
+    if spec["kind"] == "jacobi":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no Jacobi "
+                          "sweep with a right-hand side (its 3D golds are operator sweeps)"}),
+              flush=True)
+        return
     if spec["kind"] == "cnn":
         print(json.dumps({"impl": "reference", "unavailable": "the reference has no network "
                           "(the warm start is new work with no reference code)"}), flush=True)
@@ -809,6 +818,61 @@ def run_cnn(args, spec, name):
     net.close()
 
 
+def run_jacobi(args, spec, name):
+    """One step = `steps` Jacobi sweeps of -lap(u) = f on nb x n^3 in the
+    sweep storage type (the kernel both Poisson arms spend their sweeps in)."""
+    import torch
+
+    import ssam_b200 as S
+    from ssam_b200.workloads import gaussian_rhs_torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n, nb, k = spec["n"], spec["nb"], spec["steps"]
+    tdt = torch.float32 if spec["dtype"] == "f32" else torch.bfloat16
+    es = 4 if spec["dtype"] == "f32" else 2
+    rhs = gaussian_rhs_torch(nb, n, 7 + rank, dev).to(tdt)
+    u0 = torch.zeros_like(rhs)
+    out = torch.empty_like(rhs)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        S.poisson_jacobi(rhs, u0, k, u_out=out, stream=stream)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    l0 = S.lib().ssam_kernel_launches()
+    a.record(stream)
+    for _ in range(args.steps):
+        S.poisson_jacobi(rhs, u0, k, u_out=out, stream=stream)
+    b.record(stream)
+    launches = S.lib().ssam_kernel_launches() - l0
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = a.elapsed_time(b) / args.steps
+    cells = nb * n ** 3
+    peak, peak_kind = load_peaks()
+    achieved = 3 * cells * es * k / (ms / 1e3) / 1e9  # u read, rhs read, u write per sweep
+    if rank == 0:
+        print(json.dumps({
+            "metric": "GCells/s", "value": cells * k * world / (ms / 1e3) / 1e9,
+            "unit": "GCells/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": spec["dtype"], "data": "synthetic (8 Gaussian-bump right-hand sides)",
+            "config": {"workload": name, "grid": f"{nb}x{n}^3", "sweeps_per_step": k,
+                       "l2": f"u in/out + rhs: {3 * cells * es / 2**20:.0f} MiB vs 126 MB L2"},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": load_traffic(name),
+                         "algorithmic_bytes_per_launch": 3 * cells * es},
+            "clocks": clk, "e2e": None, "cpu_baseline": None,
+        }), flush=True)
+
+
 def run_ssam(args, spec, name):
     import torch
     import torch.distributed as dist
@@ -1004,6 +1068,8 @@ def main(argv=None):
         run_poisson(args, spec, args.workload)
     elif spec["kind"] == "cnn":
         run_cnn(args, spec, args.workload)
+    elif spec["kind"] == "jacobi":
+        run_jacobi(args, spec, args.workload)
     else:
         run_ssam(args, spec, args.workload)
 
