@@ -461,8 +461,11 @@ def run_batched(args, spec, name):
     ms_pg, launches_pg = timed(False, max(1, min(args.steps, 3)))
     value = cells * spec["steps"] * world / (ms / 1e3) / 1e9
     es = elem_size(spec["dtype"])
-    # phases of the persistent run: fused depth 4 (r=1) / 2 (r=2), rest single steps
+    # phases of the persistent run: fused depth 4 (r=1) / 2 (r=2), rest single
+    # steps; single steps throughout with a COPY or CLAMP boundary
     deep = 4 if r == 1 else (2 if r == 2 else 1)
+    if spec["boundary"] in ("copy", "clamp"):
+        deep = 1
     phases = spec["steps"] // deep + spec["steps"] % deep
     alg_bytes = 2 * cells * es * phases
     peak, peak_kind = load_peaks()

@@ -262,7 +262,10 @@ extern "C" int ssam_stencil2d_batched(const ssam_grid2d* grids, int ngrids, int 
   int deep = radius == 1 ? 4 : (radius == 2 ? 2 : 1);
   deep = std::min(deep, std::max(1, tune_depth_2d(dtype, radius, radius, radius, radius, star,
                                                   grids[0].width, grids[0].height, steps)));
-  if (boundary == SSAM_BOUNDARY_CLAMP) deep = 1;
+  // CLAMP is single-step only; with COPY every fused step of an edge tile
+  // reloads the fixed ring from the input, which costs more than it saves on
+  // grids this small (most warp tiles touch an edge)
+  if (boundary == SSAM_BOUNDARY_CLAMP || boundary == SSAM_BOUNDARY_COPY) deep = 1;
   while (deep > 1 && !find_batched(dtype, star, radius, deep)) deep /= 2;
   const int q = steps / deep, rem = steps % deep;
   BatchFn fn_deep = find_batched(dtype, star, radius, deep);
