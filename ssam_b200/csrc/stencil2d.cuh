@@ -165,8 +165,27 @@ __device__ __forceinline__ void stencil2d_warp_tile(
         }
       }
     }
+  } else if constexpr (T == 1) {
+    // columns beyond the left/right edge (edge lanes only): per element from
+    // clamped coordinates, zeros outside the grid for ZERO; no branches, so
+    // every load can be in flight at once (single-step windows are short
+    // enough to keep all of them in registers)
+#pragma unroll
+    for (int k = 0; k < ROWS; ++k) {
+      const int64_t y = y0 + k;
+      const bool y_out = y < 0 || y >= H;
+      const TS* row = src + (y < 0 ? 0 : (y >= H ? H - 1 : y)) * pitch;
+#pragma unroll
+      for (int j = 0; j < V; ++j) {
+        const int64_t x = x0 + j;
+        const bool out = y_out || x < 0 || x >= W;
+        const TA v = to_acc(__ldg(row + (x < 0 ? 0 : (x >= W ? W - 1 : x))));
+        d[k][j] = (out && bnd == SSAM_BOUNDARY_ZERO) ? TA(0) : v;
+      }
+    }
   } else {
-    // columns beyond the left/right edge (edge lanes only): per element
+    // the same for fused multi-step windows, one row at a time (rotated into
+    // its static slot), which keeps the register count of the deep windows
 #pragma unroll 1
     for (int k = 0; k < ROWS; ++k) {
       int64_t y = y0 + k;
@@ -178,7 +197,6 @@ __device__ __forceinline__ void stencil2d_warp_tile(
         y = y < 0 ? 0 : (y >= H ? H - 1 : y);
         load_row_edge<TS, V>(v, src + y * pitch, x0, W, bnd);
       }
-      // rotate the window so that the row can land in a static slot
 #pragma unroll
       for (int r = 0; r < ROWS - 1; ++r)
 #pragma unroll
