@@ -343,306 +343,14 @@ __global__ void __launch_bounds__(kThreads, 1) conv3d_ring_kernel(ConvArgs a) {
   if (warp == 1) tc::tmem_free(tmem, 512);
 }
 
-// ---------------------------------------------------------------------------
-// Dilation 1: the three z taps stacked into one MMA.
-//
-// tcgen05.mma costs the same ~55 cycles for every N <= 64, so with 16 output
-// channels a 128 x 16 x 16 MMA uses a fraction of the tensor pipe.  With
-// dilation 1 one input plane p feeds output planes p+1, p and p-1 through the
-// same shifted A operand and the weights of z taps 0, 1 and 2: so every
-// (dy, dx) tap of a staged plane is ONE MMA with N = 48 whose three 16-column
-// blocks are the accumulators of those three output planes.  Each input plane
-// is then staged and read once, and an output plane costs 9 MMAs per tile
-// instead of 27.  The accumulators of successive output planes rotate
-// through a ring of R blocks per tile; when the three blocks wrap around the
-// ring the MMA is split in two.  Blocks are cleared by the epilogue after it
-// has read them, so every MMA accumulates.
-constexpr int kZRing = 6;        // accumulator blocks per tile
-constexpr int kZMaxTiles = 5;    // kZRing x 16 columns x tiles <= 512
-
-struct ZPlan {
-  int ty, xp, tiles, box_rows, slab, slots, smem;
-};
-
-bool make_zplan(int n, ZPlan* p) {
-  const int dil = 1, xp = n + 1;
-  if (n > kMaxRow) return false;
-  ZPlan best{};
-  double best_eff = -1;
-  for (int ty = std::min(n, 16); ty >= 1; ty /= 2) {
-    const int box_rows = ty + 2 * dil;
-    const int tiles = (ty * xp + 127) / 128;
-    if (tiles > kZMaxTiles) continue;
-    const int tail = tiles * 128 - ty * xp + dil;
-    const int slab = ((kFrontGuard + box_rows * xp + tail) * 16 + 127) / 128 * 128;
-    const int avail = kSmemLimit - 1024 - 27 * 512 - 512;
-    const int slots = std::min(kMaxSlots, avail / (2 * slab));
-    if (slots < 3) continue;
-    const double eff = (double)ty * n / (tiles * 128.0);  // useful MMA rows
-    if (eff > best_eff + 1e-9) {
-      best_eff = eff;
-      best = ZPlan{ty, xp, tiles, box_rows, slab, slots,
-                   std::max(1024 + 27 * 512 + slots * 2 * slab + 512, 120 * 1024)};
-    }
-  }
-  if (best_eff < 0) return false;
-  *p = best;
-  return true;
-}
-
-__device__ __forceinline__ void tmem_st16_zero(uint32_t taddr) {
-  const uint32_t z = 0;
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
-      "{%1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1};" ::"r"(taddr),
-      "r"(z)
-      : "memory");
-}
-__device__ __forceinline__ void tmem_wait_st() {
-  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-}
-
-__global__ void __launch_bounds__(kThreads, 1) conv3d_zstack_kernel(ConvArgs a) {
-  constexpr uint32_t ID16 = tc::idesc_bf16(128, 16, 0, 0);
-  constexpr uint32_t ID32 = tc::idesc_bf16(128, 32, 0, 0);
-  constexpr uint32_t ID48 = tc::idesc_bf16(128, 48, 0, 0);
-  constexpr int R = kZRing;
-  extern __shared__ unsigned char smem_raw[];
-  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  unsigned char* Ws = base;  // [dy dx tap t9][dz block k = 0,1,2 -> z tap 2,1,0][512 B]
-  unsigned char* Ring = Ws + 27 * 512;
-  const int slot_bytes = 2 * a.slab;
-  const int S = a.slots;
-  uint64_t* full = (uint64_t*)(Ring + S * slot_bytes);
-  uint64_t* empty = full + kMaxSlots;
-  uint64_t* accf = empty + kMaxSlots;  // [R]
-  uint64_t* acce = accf + R;           // [R]
-  uint64_t* drain = acce + R;
-  uint32_t* tmem_slot = (uint32_t*)(drain + 1);
-
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int n = a.n, xp = a.xp;
-  const int cols_per_tile = R * 16;
-  // weights: for in-plane tap t9 = (dy+1)*3 + (dx+1), block k holds z tap 2-k
-  for (int idx = threadIdx.x; idx < 27 * 32; idx += kThreads) {
-    const int slotw = idx >> 5, co = (idx >> 1) & 15, c = idx & 1;
-    const int t9 = slotw / 3, k = slotw % 3, tap = (2 - k) * 9 + t9;
-    const uint4 v = *reinterpret_cast<const uint4*>(
-        a.w + ((size_t)co * 27 + tap) * a.ci_total + a.ci_off + c * 8);
-    *reinterpret_cast<uint4*>(Ws + slotw * 512 + (co >> 3) * 256 + c * 128 + (co & 7) * 16) = v;
-  }
-  for (int idx = threadIdx.x; idx < S * slot_bytes / 16; idx += kThreads)
-    reinterpret_cast<uint4*>(Ring)[idx] = make_uint4(0, 0, 0, 0);
-  if (threadIdx.x == 0) {
-    for (int i = 0; i < S; ++i) {
-      tc::mbar_init(&full[i], 1);
-      tc::mbar_init(&empty[i], 1);
-    }
-    for (int i = 0; i < R; ++i) {
-      tc::mbar_init(&accf[i], 1);
-      tc::mbar_init(&acce[i], 128);
-    }
-    tc::mbar_init(drain, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  if (warp == 1) tc::tmem_alloc(tmem_slot, 512);
-  tc::fence_async_smem();
-  tc::tc_fence_before();
-  __syncthreads();
-  tc::tc_fence_after();
-  const uint32_t tmem = *tmem_slot;
-  // every accumulator block starts at zero (MMAs always accumulate)
-  if (warp >= 2) {
-    const uint32_t lanes = (uint32_t)((warp & 3) * 32) << 16;
-    for (int c = 0; c < a.tiles * cols_per_tile; c += 16) tmem_st16_zero(tmem + lanes + c);
-    tmem_wait_st();
-  }
-  tc::tc_fence_before();
-  __syncthreads();
-  tc::tc_fence_after();
-
-  bool ok = true;
-  if (warp == 0) {
-    // ---------------------------------------------------------- producer
-    const uint32_t row_bytes = (uint32_t)n * 16;
-    const uint32_t plane_bytes = 2u * a.box_rows * row_bytes;
-    uint32_t gp = 0;
-    for (int64_t it = blockIdx.x; ok && it < a.items; it += gridDim.x) {
-      const Item m = decode(a, it);
-      for (int p = 0; p < m.len; ++p, ++gp) {
-        const int s = (int)(gp % S);
-        const uint32_t use = gp / S;
-        int good = 1;
-        if (lane == 0) {
-          if (use > 0 && !tc::mbar_wait(&empty[s], (use - 1) & 1, a.wait_ns)) good = 0;
-          if (good) mbar_expect_tx(&full[s], plane_bytes);
-        }
-        good = __shfl_sync(0xffffffffu, good, 0);
-        if (!good) {
-          ok = false;
-          break;
-        }
-        const int z = m.z0 - 1 + p;
-        const uint32_t bar = tc::smem_addr(&full[s]);
-        unsigned char* slot = Ring + s * slot_bytes;
-        for (int k = lane; k < 2 * a.box_rows; k += 32) {
-          const int h = k / a.box_rows, r = k % a.box_rows;
-          const int y = m.y0 - 1 + r;
-          const void* src = g_zero_row;
-          if (z >= 0 && z < n && y >= 0 && y < n)
-            src = a.in + h * a.half + ((((int64_t)m.b * n + z) * n + y) * n) * 8;
-          bulk_copy(tc::smem_addr(slot + h * a.slab + (kFrontGuard + r * xp + 1) * 16), src,
-                    row_bytes, bar);
-        }
-        __syncwarp();
-      }
-    }
-    if (lane == 0)
-      for (uint32_t k = gp > (uint32_t)S ? gp - S : 0; k < gp; ++k)
-        if (!tc::mbar_wait(&full[k % S], (k / S) & 1, a.wait_ns)) ok = false;
-  } else if (warp == 1) {
-    // ---------------------------------------------------------- MMA issuer
-    if (lane == 0) {
-      int toff[9];
-#pragma unroll
-      for (int t9 = 0; t9 < 9; ++t9) {
-        const int dy = t9 / 3 - 1, dx = t9 % 3 - 1;
-        toff[t9] = kFrontGuard + xp + dy * xp + dx;
-      }
-      const uint64_t abase0 = tc::smem_desc(Ring, (uint32_t)a.slab, 128);
-      const uint64_t wbase = tc::smem_desc(Ws, 128, 256);
-      uint32_t gp = 0, vbase = 0;
-      bool issued = false;
-      for (int64_t it = blockIdx.x; ok && it < a.items; it += gridDim.x) {
-        const Item m = decode(a, it);
-        for (int q = 0; q < m.len; ++q, ++gp) {
-          // blocks that get their first contribution here (virtual output
-          // vbase + q + 2; at the item's first plane also vbase, vbase + 1)
-          // must have been read and cleared after their previous use
-          for (uint32_t v = q == 0 ? vbase : vbase + q + 2; v <= vbase + q + 2; ++v) {
-            if (v < (uint32_t)R) continue;
-            const uint32_t u = v / R;  // use index of the block (>= 1)
-            if (!tc::mbar_wait(&acce[v % R], (u - 1) & 1, a.wait_ns)) ok = false;
-          }
-          if (!ok) break;
-          const int s = (int)(gp % S);
-          if (!tc::mbar_wait(&full[s], (gp / S) & 1, a.wait_ns)) {
-            ok = false;
-            break;
-          }
-          tc::tc_fence_after();
-          const uint64_t az = abase0 + (uint64_t)(s * (slot_bytes >> 4));
-          const int b0 = (int)((vbase + q) % R);  // block of the z-tap-2 output
-          const int c1 = b0 <= R - 3 ? 3 : R - b0;  // blocks before the wrap
-          for (int t = 0; t < a.tiles; ++t) {
-            const uint32_t dt = tmem + (uint32_t)(t * cols_per_tile);
-            const uint64_t at = az + (uint64_t)(128 * t);
-#pragma unroll
-            for (int t9 = 0; t9 < 9; ++t9) {
-              const uint64_t aa = at + (uint64_t)toff[t9];
-              const uint64_t bb = wbase + (uint64_t)(t9 * 3 * 32);
-              if (c1 == 3) {
-                tc::mma_bf16(dt + (uint32_t)(b0 * 16), aa, bb, ID48, true);
-              } else {
-                tc::mma_bf16(dt + (uint32_t)(b0 * 16), aa, bb, c1 == 1 ? ID16 : ID32, true);
-                tc::mma_bf16(dt, aa, bb + (uint64_t)(c1 * 32), c1 == 1 ? ID32 : ID16, true);
-              }
-            }
-          }
-          issued = true;
-          tc::mma_commit(&empty[s]);               // the plane is used once
-          tc::mma_commit(&accf[(vbase + q) % R]);  // its z-tap-2 output is complete
-        }
-        if (!ok) break;
-        // the two outputs past the item's last plane (invalid) are complete too
-        tc::mma_commit(&accf[(vbase + m.len) % R]);
-        tc::mma_commit(&accf[(vbase + m.len + 1) % R]);
-        vbase += m.len + 2;
-      }
-      if (issued) {
-        tc::mma_commit(drain);
-        if (!tc::mbar_wait(drain, 0, a.wait_ns)) ok = false;
-      }
-    }
-  } else {
-    // ---------------------------------------------------------- epilogue
-    const int qd = warp & 3;
-    const int row = qd * 32 + lane;
-    const uint32_t lanes = (uint32_t)(qd * 32) << 16;
-    uint32_t vbase = 0;
-    for (int64_t it = blockIdx.x; ok && it < a.items; it += gridDim.x) {
-      const Item m = decode(a, it);
-      // virtual outputs vbase + j + 2, j = -2 .. nout + 1; valid 0 <= j < nout
-      for (int j = -2; j < m.nout + 2; ++j) {
-        const uint32_t v = vbase + (uint32_t)(j + 2);
-        const int blk = (int)(v % R);
-        if (!tc::mbar_wait(&accf[blk], (v / R) & 1, a.wait_ns)) {
-          ok = false;
-          break;
-        }
-        tc::tc_fence_after();
-        const bool valid = j >= 0 && j < m.nout;
-        const int64_t zrow = ((int64_t)m.b * n + m.z0 + j) * n;
-        for (int t = 0; t < a.tiles; ++t) {
-          const uint32_t ta = tmem + lanes + (uint32_t)(t * cols_per_tile + blk * 16);
-          if (valid) {
-            float vv[16];
-            tc::tmem_ld16(ta, vv);
-            const int p = 128 * t + row;
-            const int r = p / xp, x = p % xp - 1;
-            if (r < a.ty && x >= 0 && m.y0 + r < n) {
-              const int64_t e = ((zrow + m.y0 + r) * n + x) * 8;
-#pragma unroll
-              for (int i = 0; i < 16; ++i) vv[i] *= a.out_scale;
-              if (a.addend) {
-                const uint4 u0 = *reinterpret_cast<const uint4*>(a.addend + e);
-                const uint4 u1 = *reinterpret_cast<const uint4*>(a.addend + a.half + e);
-                const __nv_bfloat16* b0 = reinterpret_cast<const __nv_bfloat16*>(&u0);
-                const __nv_bfloat16* b1 = reinterpret_cast<const __nv_bfloat16*>(&u1);
-#pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                  vv[i] += __bfloat162float(b0[i]);
-                  vv[8 + i] += __bfloat162float(b1[i]);
-                }
-              }
-              uint4 o[2];
-              __nv_bfloat16* ob = reinterpret_cast<__nv_bfloat16*>(o);
-#pragma unroll
-              for (int i = 0; i < 16; ++i) ob[i] = __float2bfloat16_rn(vv[i]);
-              *reinterpret_cast<uint4*>(a.out + e) = o[0];
-              *reinterpret_cast<uint4*>(a.out + a.half + e) = o[1];
-            }
-          }
-          tmem_st16_zero(ta);
-        }
-        tmem_wait_st();
-        tc::tc_fence_before();
-        mbar_arrive(&acce[blk]);
-      }
-      vbase += m.len + 2;
-    }
-  }
-  if (!ok) atomicCAS(a.err, 0, 8);
-  tc::tc_fence_before();
-  __syncthreads();
-  tc::tc_fence_after();
-  if (warp == 1) tc::tmem_free(tmem, 512);
-}
-
 }  // namespace
 
 // One single-source pass: out = conv(in, w[:, :, ci_off .. ci_off+15]) *
 // scale (+ addend).  SSAM_ERR_UNSUPPORTED when the shape has no plan.
 int conv3d_ring(const void* in, const void* addend, const void* w, int ci_total, int ci_off,
                 void* out, int nb, int n, int dil, float out_scale, cudaStream_t s) {
-  ZPlan zp;
-  const bool zstack = dil == 1 && make_zplan(n, &zp);
   Plan p;
-  if (zstack) {
-    p = Plan{zp.ty, zp.xp, zp.tiles, zp.box_rows, zp.slab, zp.slots, zp.smem};
-  } else if (!make_plan(n, dil, &p)) {
-    return SSAM_ERR_UNSUPPORTED;
-  }
+  if (!make_plan(n, dil, &p)) return SSAM_ERR_UNSUPPORTED;
   ConvArgs a;
   a.in = (const __nv_bfloat16*)in;
   a.addend = (const __nv_bfloat16*)addend;
@@ -674,7 +382,7 @@ int conv3d_ring(const void* in, const void* addend, const void* w, int ci_total,
     const int zc = (n + nzc - 1) / nzc;
     const int64_t items = cols * nzc;
     const int64_t rounds = (items + sms - 1) / sms;
-    const int64_t cost = rounds * (dil == 1 ? zc + 2 : 3 * zc);  // planes staged per item
+    const int64_t cost = rounds * (dil == 1 ? zc + 2 : 3 * zc);
     if (best < 0 || cost < best) {
       best = cost;
       a.nzc = nzc;
@@ -686,15 +394,10 @@ int conv3d_ring(const void* in, const void* addend, const void* w, int ci_total,
   if (!attr_set) {
     SSAM_CUDA_TRY(cudaFuncSetAttribute(conv3d_ring_kernel,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimit));
-    SSAM_CUDA_TRY(cudaFuncSetAttribute(conv3d_zstack_kernel,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimit));
     attr_set = true;
   }
   const int64_t grid = std::min<int64_t>(a.items, sms);
-  if (zstack)
-    conv3d_zstack_kernel<<<(unsigned)grid, kThreads, p.smem, s>>>(a);
-  else
-    conv3d_ring_kernel<<<(unsigned)grid, kThreads, p.smem, s>>>(a);
+  conv3d_ring_kernel<<<(unsigned)grid, kThreads, p.smem, s>>>(a);
   count_launch();
   SSAM_CUDA_TRY(cudaGetLastError());
   return SSAM_OK;
