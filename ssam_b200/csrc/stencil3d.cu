@@ -71,11 +71,13 @@ struct Launch3D {
   bool prepare_only;  // resolve attributes/occupancy/symbols, launch nothing
 };
 
-template <typename TS, int SH, int R, int PY, int NW, int S>
+template <typename TS, int SH, int R, int PY, int NW, int S, bool RHS = false>
 static int launch_3d(const Launch3D& a) {
   using C = Stencil3DCfg<TS, SH, R, PY, NW, S>;
   using TA = typename C::TA;
-  auto kern = stencil3d_kernel<TS, SH, R, PY, NW, S>;
+  auto kern = stencil3d_kernel<TS, SH, R, PY, NW, S, RHS>;
+  if ((a.rhs != nullptr) != RHS)
+    return fail(SSAM_ERR_INVALID, "3D kernel instance does not match the right-hand side");
   static std::mutex mu;
   static std::map<int, int> ctas_per_sm;  // per device
   int dev = 0;
@@ -185,6 +187,16 @@ static LaunchFn3D find_3d(int dtype, int shape, int r) {
       case SSAM_BF16: return &launch_3d<__nv_bfloat16, SH3_POISSON19, 1, 4, 8, 6>;
       case SSAM_F16: return &launch_3d<__half, SH3_POISSON19, 1, 4, 8, 6>;
     }
+  }
+  return nullptr;
+}
+
+// The 7-point instances with the right-hand-side term (the Jacobi sweep).
+static LaunchFn3D find_3d_rhs(int dtype) {
+  switch (dtype) {
+    case SSAM_F32: return &launch_3d<float, SH3_STAR, 1, 4, 8, 6, true>;
+    case SSAM_F64: return &launch_3d<double, SH3_STAR, 1, 4, 4, 5, true>;
+    case SSAM_BF16: return &launch_3d<__nv_bfloat16, SH3_STAR, 1, 4, 8, 6, true>;
   }
   return nullptr;
 }
@@ -347,7 +359,7 @@ namespace ssam {
 // (Dirichlet) boundary.  Used by the Poisson Jacobi sweeps.
 int sweep_3d(const void* in, void* out, int64_t n, int nb, int dtype, const double* cube,
              const void* rhs, double rhs_scale, cudaStream_t s) {
-  LaunchFn3D fn = find_3d(dtype, SH3_STAR, 1);
+  LaunchFn3D fn = rhs ? find_3d_rhs(dtype) : find_3d(dtype, SH3_STAR, 1);
   if (!fn) return fail(SSAM_ERR_UNSUPPORTED, "no 3D 7-point kernel for this dtype");
   Launch3D a{in, out, n, n, n, nb, rhs, rhs_scale, cube, SSAM_BOUNDARY_ZERO, s, false};
   return fn(a);

@@ -214,7 +214,10 @@ __device__ __forceinline__ Seg3D item_seg(int64_t it, const Work3D& w) {
   return s;
 }
 
-template <typename TS, int SH, int R, int PY, int NW, int S>
+// RHS: the Jacobi form out = stencil(in) + rhs_scale * rhs.  Its rows are
+// loaded at the top of every plane, so their latency overlaps the plane's
+// barrier waits and arithmetic (instances without it carry no rhs code).
+template <typename TS, int SH, int R, int PY, int NW, int S, bool RHS = false>
 __global__ void __launch_bounds__(32 * (NW + 1), 2)
 stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__ src,
                  TS* __restrict__ dst, Work3D w,
@@ -307,6 +310,22 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
     for (int64_t z = sg.za; z < sg.zb; ++z) {
       // planes z-R .. z+R sit at ring positions n + (z - za) .. + 2R
       const uint32_t q0 = n + (uint32_t)(z - sg.za);
+      TA frh[RHS ? PY : 1][V];
+      if constexpr (RHS) {
+        constexpr int VB = V * (int)sizeof(TS);
+#pragma unroll
+        for (int i = 0; i < PY; ++i) {
+          const int64_t y = y0 + i;
+          const TS* fp = (const TS*)w.rhs + (sg.b * nz + z) * nxy + y * nx + x0;
+          if (y < ny && x0 + V <= nx && ((uintptr_t)fp % (VB >= 16 ? 16 : 8)) == 0) {
+            load_slot_row<TS, V>(frh[i], fp);
+          } else {
+#pragma unroll
+            for (int j = 0; j < V; ++j)
+              frh[i][j] = (y < ny && x0 + j < nx) ? to_acc(fp[j]) : TA(0);
+          }
+        }
+      }
       bool ok = true;
 #pragma unroll
       for (int k = 0; k < F; ++k) {
@@ -420,18 +439,9 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
         TA o[V];
 #pragma unroll
         for (int j = 0; j < V; ++j) o[j] = acc[i][j];
-        if (w.rhs) {
-          // Jacobi form: out = stencil(in) + rhs_scale * rhs
-          const TS* fp = (const TS*)w.rhs + cell;
-          TA f[V];
-          if (vec && ((uintptr_t)fp % (VB >= 16 ? 16 : 8)) == 0) {
-            load_slot_row<TS, V>(f, fp);
-          } else {
+        if constexpr (RHS) {
 #pragma unroll
-            for (int j = 0; j < V; ++j) f[j] = x0 + j < nx ? to_acc(fp[j]) : TA(0);
-          }
-#pragma unroll
-          for (int j = 0; j < V; ++j) o[j] = fma((TA)w.rhs_scale, f[j], o[j]);
+          for (int j = 0; j < V; ++j) o[j] = fma((TA)w.rhs_scale, frh[i][j], o[j]);
         }
         if (any_ring) {
 #pragma unroll
