@@ -407,11 +407,12 @@ def run_batched(args, spec, name):
     (value) against one launch chain per grid (reported beside it)."""
     import torch
     import ssam_b200 as S
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
+    from ssam_b200 import shard
+    r = shard.ranks()
+    rank, world, local = r.rank, r.world, r.local
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    shard.init("nccl", 300, dev)
     tdt = {"f32": torch.float32, "f64": torch.float64, "bf16": torch.bfloat16}[spec["dtype"]]
     sides = batch_sides(spec)
     gen = torch.Generator(device=dev)
@@ -455,9 +456,11 @@ def run_batched(args, spec, name):
         return a.elapsed_time(b) / k, (l1 - l0) // k
 
     clocks = ClockSampler(local)
+    shard.barrier()
     clocks.start()
     ms, launches = timed(True, args.steps)
     clk = clocks.stop()
+    ms = shard.max_over_ranks(ms, dev)
     ms_pg, launches_pg = timed(False, max(1, min(args.steps, 3)))
     value = cells * spec["steps"] * world / (ms / 1e3) / 1e9
     es = elem_size(spec["dtype"])
@@ -518,6 +521,7 @@ def run_batched(args, spec, name):
                     "steps": k_e2e},
             "cpu_baseline": cpu,
         }), flush=True)
+    shard.finish()
 
 
 def batched_cpu_baseline(spec, sides, budget_s=10.0):
@@ -556,21 +560,17 @@ def run_poisson(args, spec, name):
     events around the solve; the solve itself reads FP64 residual norms on
     the host between corrections)."""
     import torch
-    import torch.distributed as dist
 
     import oracle
     import ssam_b200 as S
+    from ssam_b200 import shard
     from ssam_b200.workloads import gaussian_rhs_torch
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    r = shard.ranks()
+    rank, world, local = r.rank, r.world, r.local
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=dev)
+    shard.init("nccl", 300, dev)
     n, nb, tol = spec["n"], spec["nb"], spec["tol"]
     f = gaussian_rhs_torch(nb, n, 7 + rank, dev)
     stream = torch.cuda.current_stream(dev)
@@ -589,8 +589,7 @@ def run_poisson(args, spec, name):
     for _ in range(args.warmup):
         solve(opts)
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    shard.barrier()
     clocks = ClockSampler(local)
     clocks.start()
     times, stats = [], []
@@ -606,11 +605,7 @@ def run_poisson(args, spec, name):
         stats.append(st)
     launches = S.lib().ssam_kernel_launches() - launches0
     clk = clocks.stop()
-    sec = sum(times) / len(times)
-    if world > 1:
-        t = torch.tensor([sec], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        sec = t.item()
+    sec = shard.max_over_ranks(sum(times) / len(times), dev)
     # FP64 check of the last answer: the library's residual and the oracle's
     check_gpu = max(S.poisson_residual(f, u))
     f_np = f.cpu().numpy()
@@ -736,8 +731,7 @@ def run_poisson(args, spec, name):
         }), flush=True)
     if net is not None:
         net.close()
-    if world > 1:
-        dist.destroy_process_group()
+    shard.finish()
 
 
 def cnn_forward_flops(n, nb):
@@ -752,12 +746,13 @@ def run_cnn(args, spec, name):
     import torch
 
     import ssam_b200 as S
+    from ssam_b200 import shard
     from ssam_b200.workloads import gaussian_rhs_torch
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
+    r = shard.ranks()
+    rank, world, local = r.rank, r.world, r.local
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    shard.init("nccl", 120, dev)
     n, nb = spec["n"], spec["nb"]
     f = gaussian_rhs_torch(nb, n, 7 + rank, dev)
     net = S.WarmStartCNN(n, nb)
@@ -779,7 +774,7 @@ def run_cnn(args, spec, name):
     launches = S.lib().ssam_kernel_launches() - l0
     torch.cuda.synchronize()
     clk = clocks.stop()
-    ms = a.elapsed_time(b) / args.steps
+    ms = shard.max_over_ranks(a.elapsed_time(b) / args.steps, dev)
     flops = cnn_forward_flops(n, nb)
     value = flops / (ms / 1e3) / 1e12 * world
     try:
@@ -819,6 +814,7 @@ def run_cnn(args, spec, name):
             "cpu_baseline": None,
         }), flush=True)
     net.close()
+    shard.finish()
 
 
 def run_jacobi(args, spec, name):
@@ -827,12 +823,13 @@ def run_jacobi(args, spec, name):
     import torch
 
     import ssam_b200 as S
+    from ssam_b200 import shard
     from ssam_b200.workloads import gaussian_rhs_torch
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
+    r = shard.ranks()
+    rank, world, local = r.rank, r.world, r.local
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    shard.init("nccl", 120, dev)
     n, nb, k = spec["n"], spec["nb"], spec["steps"]
     tdt = torch.float32 if spec["dtype"] == "f32" else torch.bfloat16
     es = 4 if spec["dtype"] == "f32" else 2
@@ -855,7 +852,7 @@ def run_jacobi(args, spec, name):
     launches = S.lib().ssam_kernel_launches() - l0
     torch.cuda.synchronize()
     clk = clocks.stop()
-    ms = a.elapsed_time(b) / args.steps
+    ms = shard.max_over_ranks(a.elapsed_time(b) / args.steps, dev)
     cells = nb * n ** 3
     peak, peak_kind = load_peaks()
     achieved = 3 * cells * es * k / (ms / 1e3) / 1e9  # u read, rhs read, u write per sweep
@@ -874,23 +871,20 @@ def run_jacobi(args, spec, name):
                          "algorithmic_bytes_per_launch": 3 * cells * es},
             "clocks": clk, "e2e": None, "cpu_baseline": None,
         }), flush=True)
+    shard.finish()
 
 
 def run_ssam(args, spec, name):
     import torch
-    import torch.distributed as dist
 
     import ssam_b200 as S
+    from ssam_b200 import shard
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    r = shard.ranks()
+    rank, world, local = r.rank, r.world, r.local
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=dev)
+    shard.init("nccl", 120, dev)
 
     n = spec["n"]
     kind = spec["kind"]
@@ -923,9 +917,7 @@ def run_ssam(args, spec, name):
             S.stencil2d(srcs[i % 2], c, r, shape, steps=spec["steps"],
                         boundary=spec["boundary"], dst=dst, stream=stream)
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
+    barrier = shard.barrier
 
     # the project's autotuner picks P, strip width, warps and temporal depth
     # for this stencil and grid size (outside the timed region)
@@ -964,10 +956,7 @@ def run_ssam(args, spec, name):
     total_ms = t_start.elapsed_time(t_end)
     launch_ms = [a.elapsed_time(b) for a, b in ev]
     avg_launch_ms = sum(launch_ms) / len(launch_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = t.item()
+    total_ms = shard.max_over_ranks(total_ms, dev)
 
     cells = n ** len(dims) * spec["steps"]
     value = cells * args.steps * world / (total_ms / 1e3) / 1e9
@@ -998,11 +987,7 @@ def run_ssam(args, spec, name):
             host_call(hs, hd, c, r, shape, spec["steps"], spec["boundary"], dev, stream)
         b.record(stream)
         torch.cuda.synchronize()
-        e_ms = a.elapsed_time(b)
-        if world > 1:
-            t = torch.tensor([e_ms], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_ms = t.item()
+        e_ms = shard.max_over_ranks(a.elapsed_time(b), dev)
         e2e = {"value": cells * k_e2e * world / (e_ms / 1e3) / 1e9, "unit": "GCells/s",
                "h2d_bytes_per_step": n ** len(dims) * es,
                "d2h_bytes_per_step": n ** len(dims) * es,
@@ -1044,8 +1029,7 @@ def run_ssam(args, spec, name):
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    shard.finish()
 
 
 def main(argv=None):

@@ -1,0 +1,82 @@
+"""The multi-rank plumbing of the benchmark (ssam_b200/shard.py) with two
+gloo ranks on the CPU: the process group forms over 127.0.0.1, the timing
+reduction returns the slowest rank's time on every rank, work partitions
+cover every unit once, and a rank that never joins makes the others fail
+within the short group timeout instead of hanging."""
+import os
+import socket
+import subprocess
+import sys
+
+import pytest
+
+from ssam_b200 import shard
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+WORKER = r"""
+import os, sys, json
+sys.path.insert(0, {root!r})
+from ssam_b200 import shard
+r = shard.init("gloo", timeout_s={timeout})
+shard.barrier()
+t = shard.max_over_ranks(0.5 + r.rank)
+part = list(shard.partition(10, r.rank, r.world))
+print(json.dumps({{"rank": r.rank, "world": r.world, "max": t, "part": part}}), flush=True)
+shard.finish()
+"""
+
+
+def launch(world, port, timeout=20, only=None):
+    procs = []
+    for rank in range(world):
+        if only is not None and rank not in only:
+            continue
+        env = dict(os.environ, RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank),
+                   MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        procs.append(subprocess.Popen(
+            [sys.executable, "-c", WORKER.format(root=ROOT, timeout=timeout)], env=env,
+            stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+    return procs
+
+
+def test_two_gloo_ranks_share_the_slowest_time_and_partition_the_units():
+    import json
+    procs = launch(2, free_port())
+    outs = []
+    for p in procs:
+        out, err = p.communicate(timeout=120)
+        assert p.returncode == 0, err
+        outs.append(json.loads(out.strip().splitlines()[-1]))
+    assert sorted(o["rank"] for o in outs) == [0, 1]
+    assert all(o["world"] == 2 and o["max"] == 1.5 for o in outs)
+    units = sorted(u for o in outs for u in o["part"])
+    assert units == list(range(10))
+
+
+def test_a_missing_rank_fails_the_others_instead_of_hanging():
+    procs = launch(2, free_port(), timeout=5, only={0})
+    out, err = procs[0].communicate(timeout=180)
+    assert procs[0].returncode != 0
+
+
+@pytest.mark.parametrize("n,world", [(10, 3), (3, 4), (256, 8), (0, 2)])
+def test_partition_is_balanced_and_complete(n, world):
+    parts = [shard.partition(n, r, world) for r in range(world)]
+    sizes = [len(p) for p in parts]
+    assert sum(sizes) == n and max(sizes) - min(sizes) <= 1
+    assert [u for p in parts for u in p] == list(range(n))
+
+
+def test_single_rank_needs_no_group():
+    r = shard.ranks()
+    assert shard.max_over_ranks(3.25) == 3.25
+    assert shard.weak_rate(100.0, 4, 2.0) == 200.0
+    assert r.world >= 1
