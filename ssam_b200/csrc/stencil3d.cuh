@@ -307,23 +307,51 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
     // does my strip touch the x/y ring that COPY keeps?
     const bool ring_xy = w.boundary == SSAM_BOUNDARY_COPY &&
                          (x0 < R || x0 + V > nx - R || y0 < R || y0 + PY > ny - R);
+    // right-hand side rows, kept as raw 32-bit words: 2-byte types load plane
+    // z+1 while plane z is computed (software pipelined across the z loop);
+    // wider types load plane z at the top of its iteration (registers)
+    constexpr int RW = V * (int)sizeof(TS) / 4;  // words per rhs row
+    constexpr bool PIPE = sizeof(TS) == 2;
+    uint32_t rawc[RHS ? PY : 1][RW];
+    uint32_t rawn[(RHS && PIPE) ? PY : 1][RW];
+    auto load_rhs = [&](int64_t zz, uint32_t (&dst)[RHS ? PY : 1][RW]) {
+#pragma unroll
+      for (int i = 0; i < (RHS ? PY : 1); ++i) {
+        const int64_t y = y0 + i;
+        const TS* fp = (const TS*)w.rhs + (sg.b * nz + zz) * nxy + y * nx + x0;
+        if (y < ny && x0 + V <= nx && ((uintptr_t)fp % (RW >= 4 ? 16 : 8)) == 0) {
+          if constexpr (RW == 2) {
+            const uint2 v = __ldg(reinterpret_cast<const uint2*>(fp));
+            dst[i][0] = v.x;
+            dst[i][1] = v.y;
+          } else {
+#pragma unroll
+            for (int c = 0; c < RW / 4; ++c) {
+              const uint4 v = __ldg(reinterpret_cast<const uint4*>(fp) + c);
+              dst[i][4 * c] = v.x;
+              dst[i][4 * c + 1] = v.y;
+              dst[i][4 * c + 2] = v.z;
+              dst[i][4 * c + 3] = v.w;
+            }
+          }
+        } else {
+          TS tmp[V];
+#pragma unroll
+          for (int j = 0; j < V; ++j)
+            tmp[j] = (y < ny && x0 + j < nx) ? fp[j] : from_acc<TS>(TA(0));
+          memcpy(dst[i], tmp, sizeof(tmp));
+        }
+      }
+    };
+    if constexpr (RHS && PIPE) load_rhs(sg.za, rawc);
     for (int64_t z = sg.za; z < sg.zb; ++z) {
       // planes z-R .. z+R sit at ring positions n + (z - za) .. + 2R
       const uint32_t q0 = n + (uint32_t)(z - sg.za);
-      TA frh[RHS ? PY : 1][V];
       if constexpr (RHS) {
-        constexpr int VB = V * (int)sizeof(TS);
-#pragma unroll
-        for (int i = 0; i < PY; ++i) {
-          const int64_t y = y0 + i;
-          const TS* fp = (const TS*)w.rhs + (sg.b * nz + z) * nxy + y * nx + x0;
-          if (y < ny && x0 + V <= nx && ((uintptr_t)fp % (VB >= 16 ? 16 : 8)) == 0) {
-            load_slot_row<TS, V>(frh[i], fp);
-          } else {
-#pragma unroll
-            for (int j = 0; j < V; ++j)
-              frh[i][j] = (y < ny && x0 + j < nx) ? to_acc(fp[j]) : TA(0);
-          }
+        if constexpr (PIPE) {
+          if (z + 1 < sg.zb) load_rhs(z + 1, rawn);
+        } else {
+          load_rhs(z, rawc);
         }
       }
       bool ok = true;
@@ -440,8 +468,10 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
 #pragma unroll
         for (int j = 0; j < V; ++j) o[j] = acc[i][j];
         if constexpr (RHS) {
+          TS fv[V];
+          memcpy(fv, rawc[i], sizeof(fv));
 #pragma unroll
-          for (int j = 0; j < V; ++j) o[j] = fma((TA)w.rhs_scale, frh[i][j], o[j]);
+          for (int j = 0; j < V; ++j) o[j] = fma((TA)w.rhs_scale, to_acc(fv[j]), o[j]);
         }
         if (any_ring) {
 #pragma unroll
@@ -458,6 +488,12 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
           for (int j = 0; j < V; ++j)
             if (x0 + j < nx) outp[j] = from_acc<TS>(o[j]);
         }
+      }
+      if constexpr (RHS && PIPE) {
+#pragma unroll
+        for (int i = 0; i < PY; ++i)
+#pragma unroll
+          for (int c = 0; c < RW; ++c) rawc[i][c] = rawn[i][c];
       }
     }
     n += (uint32_t)seg_planes;
