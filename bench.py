@@ -969,6 +969,21 @@ def run_ssam(args, spec, name):
     achieved = alg_bytes / (avg_launch_ms / 1e3) / 1e9
     traffic = load_traffic(name)
 
+    # reduced-precision 3D runs: max / RMS error of the last call's result
+    # against the same run in FP64 (the FP64 kernel matches the CPU oracle to
+    # 1e-12 in the tests), outside the timed region
+    err = None
+    if kind == "3d" and spec["dtype"] != "f64":
+        i_last = (args.steps - 1) % 2
+        ref = S.stencil3d(srcs[i_last].double(), c, r, shape, steps=spec["steps"],
+                          boundary=spec["boundary"], stream=stream)
+        d = dst.double() - ref
+        err = {"max_abs": d.abs().max().item(), "rms": d.pow(2).mean().sqrt().item(),
+               "max_rel_to_range": (d.abs().max() / ref.abs().max()).item(),
+               "reference": "the same steps in FP64 on the GPU (FP64 kernel = CPU oracle "
+                            "to 1e-12 in tests/test_stencil3d_gpu.py)"}
+        del ref, d
+
     # end to end: host buffers through ssam_stencil2d_host, copies timed
     e2e = None
     if kind != "conv":
@@ -1028,6 +1043,8 @@ def run_ssam(args, spec, name):
             "e2e": e2e,
             "cpu_baseline": cpu,
         }
+        if err is not None:
+            line["error_vs_fp64"] = err
         print(json.dumps(line), flush=True)
     shard.finish()
 
