@@ -80,3 +80,48 @@ def test_single_rank_needs_no_group():
     assert shard.max_over_ranks(3.25) == 3.25
     assert shard.weak_rate(100.0, 4, 2.0) == 200.0
     assert r.world >= 1
+
+
+SLAB_WORKER = r"""
+import os, sys, json
+sys.path.insert(0, {root!r})
+import numpy as np, torch
+import oracle
+from ssam_b200 import shard, slab
+r = shard.init("gloo", timeout_s=30)
+H, W, radius, steps, depth = {H}, {W}, {radius}, {steps}, {depth}
+g = np.random.Generator(np.random.PCG64(5))
+grid = g.uniform(-1, 1, size=(H, W))
+m = g.random((2 * radius + 1, 2 * radius + 1)); m /= m.sum()
+mine = shard.partition(H, r.rank, r.world)
+local = torch.from_numpy(grid[mine.start:mine.stop].copy())
+# the oracle stands in for the GPU kernel on the extended band (test only)
+compute = lambda ext, t: torch.from_numpy(oracle.conv2d(ext.numpy(), m, "zero", steps=t))
+out = slab.run(local, H, radius, steps, depth, compute)
+want = oracle.conv2d(grid, m, "zero", steps=steps)[mine.start:mine.stop]
+print(json.dumps({{"rank": r.rank, "maxerr": float(np.abs(out.numpy() - want).max())}}),
+      flush=True)
+shard.finish()
+"""
+
+
+@pytest.mark.parametrize("world,H,radius,steps,depth", [(2, 40, 1, 5, 2), (3, 31, 2, 4, 4),
+                                                         (2, 12, 2, 3, 1)])
+def test_row_slabs_with_halo_exchange_match_the_whole_grid(world, H, radius, steps, depth):
+    """Row slabs over gloo ranks, halos of radius * depth rows swapped before
+    every temporal block: each rank's rows equal the same steps on the whole
+    grid (bit for bit: the same arithmetic on the same values)."""
+    import json
+    port = free_port()
+    procs = []
+    for rank in range(world):
+        env = dict(os.environ, RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank),
+                   MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        code = SLAB_WORKER.format(root=ROOT, H=H, W=23, radius=radius, steps=steps, depth=depth)
+        procs.append(subprocess.Popen([sys.executable, "-c", code], env=env,
+                                      stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+    for p in procs:
+        out, err = p.communicate(timeout=180)
+        assert p.returncode == 0, err
+        res = json.loads(out.strip().splitlines()[-1])
+        assert res["maxerr"] == 0.0, res
