@@ -969,20 +969,28 @@ def run_ssam(args, spec, name):
     achieved = alg_bytes / (avg_launch_ms / 1e3) / 1e9
     traffic = load_traffic(name)
 
-    # reduced-precision 3D runs: max / RMS error of the last call's result
-    # against the same run in FP64 (the FP64 kernel matches the CPU oracle to
-    # 1e-12 in the tests), outside the timed region
+    # reduced-precision runs: max / RMS error of the last call's result
+    # against the same call in FP64 on the same stored inputs (the FP64
+    # kernels match the CPU oracle to 1e-12 in the tests), outside the timed
+    # region
     err = None
-    if kind == "3d" and spec["dtype"] != "f64":
+    if spec["dtype"] != "f64":
         i_last = (args.steps - 1) % 2
-        ref = S.stencil3d(srcs[i_last].double(), c, r, shape, steps=spec["steps"],
-                          boundary=spec["boundary"], stream=stream)
+        x64 = srcs[i_last].double()
+        if kind == "3d":
+            ref = S.stencil3d(x64, c, r, shape, steps=spec["steps"],
+                              boundary=spec["boundary"], stream=stream)
+        elif kind == "conv":
+            ref = S.conv2d(x64, w, boundary=spec["boundary"], stream=stream)
+        else:
+            ref = S.stencil2d(x64, c, r, shape, steps=spec["steps"],
+                              boundary=spec["boundary"], stream=stream)
         d = dst.double() - ref
         err = {"max_abs": d.abs().max().item(), "rms": d.pow(2).mean().sqrt().item(),
                "max_rel_to_range": (d.abs().max() / ref.abs().max()).item(),
-               "reference": "the same steps in FP64 on the GPU (FP64 kernel = CPU oracle "
-                            "to 1e-12 in tests/test_stencil3d_gpu.py)"}
-        del ref, d
+               "reference": "the same call in FP64 on the GPU on the same stored inputs "
+                            "(FP64 kernels = CPU oracle to 1e-12 in tests/)"}
+        del ref, d, x64
 
     # end to end: host buffers through ssam_stencil2d_host, copies timed
     e2e = None
