@@ -581,6 +581,11 @@ def run_poisson(args, spec, name):
         net.load(CNN_WEIGHTS)
         opts["cnn"] = net
     u = torch.zeros_like(f)
+    # the autotuner picks the sweep kernel's tile and ring for this batch size
+    # (both sweep precisions: the learned arm's line also times the plain arm)
+    tuned = None
+    if not args.no_autotune:
+        tuned = {dt: S.autotune_jacobi3d(n, nb, dt, dev, stream) for dt in ("f32", "bf16")}
 
     def solve(o):
         u.zero_()
@@ -713,7 +718,7 @@ def run_poisson(args, spec, name):
             "vs_baseline": None, "dtype": f"f64 residual/correction, {sweep_dt} sweeps"
             + (", bf16 CNN" if net is not None else ""),
             "data": "synthetic (8 Gaussian-bump right-hand sides, seed 7)",
-            "config": {"workload": name, "grid": f"{nb}x{n}^3", "tol": tol,
+            "config": {"workload": name, "grid": f"{nb}x{n}^3", "tol": tol, "tuned": tuned,
                        "arm": spec["arm"], **{k: v for k, v in opts.items() if k != "cnn"},
                        "weights": os.path.relpath(CNN_WEIGHTS, ROOT) if net else None,
                        "parallelism": f"dp{world} (independent right-hand sides per GPU)",
@@ -837,6 +842,7 @@ def run_jacobi(args, spec, name):
     u0 = torch.zeros_like(rhs)
     out = torch.empty_like(rhs)
     stream = torch.cuda.current_stream(dev)
+    tuned = None if args.no_autotune else S.autotune_jacobi3d(n, nb, spec["dtype"], dev, stream)
     for _ in range(args.warmup):
         S.poisson_jacobi(rhs, u0, k, u_out=out, stream=stream)
     torch.cuda.synchronize()
@@ -863,6 +869,7 @@ def run_jacobi(args, spec, name):
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": spec["dtype"], "data": "synthetic (8 Gaussian-bump right-hand sides)",
             "config": {"workload": name, "grid": f"{nb}x{n}^3", "sweeps_per_step": k,
+                       "tuned": tuned,
                        "l2": f"u in/out + rhs: {3 * cells * es / 2**20:.0f} MiB vs 126 MB L2"},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -922,6 +929,10 @@ def run_ssam(args, spec, name):
     # the project's autotuner picks P, strip width, warps and temporal depth
     # for this stencil and grid size (outside the timed region)
     tuned = None
+    if not args.no_autotune and kind == "3d":
+        # the 3D autotuner picks rows per warp, consumer warps and ring depth
+        tuned = S.autotune_stencil3d(srcs[0], c, r, shape, boundary=spec["boundary"], dst=dst,
+                                     stream=stream)
     if not args.no_autotune and kind in ("box", "star") or (kind == "conv" and spec["f"] % 2):
         coeffs_for_tune = list(np.ravel(c)) if kind != "conv" else list(w.ravel())
         tune_shape = shape if kind != "conv" else S.BOX

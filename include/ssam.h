@@ -260,7 +260,41 @@ SSAM_API int ssam_autotune_stencil2d(const void* src, void* dst, int64_t width,
                                      int radius, const double* coeffs, int steps,
                                      int boundary, void* stream, ssam_tune_report* report);
 
-/* Persist / restore / forget the measured choices (a small text file). */
+/* What the 3D autotuner chose for one stencil and grid size. */
+typedef struct ssam_tune3d_report {
+  int rows_per_warp;  /* PY: rows of the column tile each consumer warp computes */
+  int consumer_warps; /* NW: consumer warps per CTA; the tile is 128 x NW*PY cells */
+  int ring_slots;     /* S: z-planes of the tile staged in shared memory */
+  int candidates;     /* configurations timed */
+  double ms_per_step; /* best measured time of one launch (ms) */
+} ssam_tune3d_report;
+
+/*
+ * Times every compiled configuration of this 3D stencil (rows per warp,
+ * consumer warps, shared-memory ring depth) for one step on the caller's
+ * buffers (dst is overwritten) and stores the fastest for the grid's size
+ * class (log2 of nx, ny, nz); later ssam_stencil3d / _host calls on grids of
+ * that class use it (cached step graphs are re-captured).  The reference
+ * fixes these per GPU model (BLOCK_SIZE / PROCESS_DATA_COUNT chosen with
+ * IsTeslaV100(), tmp3d7pt-v2.cu:341-387).  Synchronous.  `report` may be NULL.
+ */
+SSAM_API int ssam_autotune_stencil3d(const void* src, void* dst, int64_t nx, int64_t ny,
+                                     int64_t nz, int dtype, int shape, int radius,
+                                     const double* coeffs, int boundary, void* stream,
+                                     ssam_tune3d_report* report);
+
+/*
+ * The same for the Jacobi sweep of the Poisson solver (7-point stencil plus
+ * right-hand-side term) on `nbatch` stacked n^3 grids stored as sweep_dtype
+ * (SSAM_F32 or SSAM_BF16); times on scratch buffers of its own (stream-ordered
+ * pool), so it needs no caller data.  Later ssam_poisson_solve* calls of that
+ * size use the choice.
+ */
+SSAM_API int ssam_autotune_jacobi3d(int64_t n, int nbatch, int sweep_dtype, void* stream,
+                                    ssam_tune3d_report* report);
+
+/* Persist / restore / forget the measured choices of the 2D and 3D
+ * autotuners (a small text file). */
 SSAM_API int ssam_autotune_save(const char* path);
 SSAM_API int ssam_autotune_load(const char* path);
 SSAM_API int ssam_autotune_clear(void);

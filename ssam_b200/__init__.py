@@ -120,6 +120,11 @@ def _declare(lib):
         getattr(lib, name).restype = _int
         getattr(lib, name).argtypes = [ctypes.c_char_p]
     lib.ssam_autotune_clear.restype = _int
+    lib.ssam_autotune_stencil3d.restype = _int
+    lib.ssam_autotune_stencil3d.argtypes = [_vp, _vp, _i64, _i64, _i64, _int, _int, _int, _dp,
+                                            _int, _vp, _vp]
+    lib.ssam_autotune_jacobi3d.restype = _int
+    lib.ssam_autotune_jacobi3d.argtypes = [_i64, _int, _int, _vp, _vp]
     lib.ssam_conv2d.restype = _int
     lib.ssam_conv2d.argtypes = [_vp, _vp, _i64, _i64, _i64, _int, _dp, _int, _int,
                                 _int, _vp]
@@ -372,6 +377,50 @@ def autotune_stencil2d(src, coeffs, radius: int, shape: int = STAR, steps: int =
                                          _dtype_code(src), shape, radius, _doubles(coeffs),
                                          steps, BOUNDARY[boundary], _stream_ptr(src, stream),
                                          ctypes.byref(rep)))
+    return rep.as_dict()
+
+
+class Tune3DReport(ctypes.Structure):
+    """``ssam_tune3d_report``."""
+    _fields_ = [("rows_per_warp", ctypes.c_int), ("consumer_warps", ctypes.c_int),
+                ("ring_slots", ctypes.c_int), ("candidates", ctypes.c_int),
+                ("ms_per_step", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def autotune_stencil3d(src, coeffs, radius: int = 1, shape: int = STAR3D,
+                       boundary: str = "zero", dst=None, stream=None) -> dict:
+    """Measure every compiled 3D configuration for one step on ``src``
+    (``dst`` is scratch) and keep the fastest for this grid size class
+    (``ssam_autotune_stencil3d``)."""
+    dst = _grid3d(src, dst)
+    nz, ny, nx = src.shape
+    flat = coeffs.ravel().tolist() if hasattr(coeffs, "ravel") else list(coeffs)
+    rep = Tune3DReport()
+    _check(lib().ssam_autotune_stencil3d(src.data_ptr(), dst.data_ptr(), nx, ny, nz,
+                                         _dtype_code(src), shape, radius, _doubles(flat),
+                                         BOUNDARY[boundary], _stream_ptr(src, stream),
+                                         ctypes.byref(rep)))
+    return rep.as_dict()
+
+
+def autotune_jacobi3d(n: int, nbatch: int, sweep_dtype: str = "f32", device=None,
+                      stream=None) -> dict:
+    """Measure the Poisson solver's Jacobi-sweep configurations for `nbatch`
+    stacked n^3 grids (``ssam_autotune_jacobi3d``; scratch buffers of its
+    own); later solves of that size use the fastest."""
+    import torch
+    dev = torch.device(device) if device is not None else torch.device(
+        "cuda", torch.cuda.current_device())
+    if stream is None:
+        stream = torch.cuda.current_stream(dev)
+    code = {"f32": F32, "bf16": BF16}[sweep_dtype]
+    rep = Tune3DReport()
+    with torch.cuda.device(dev):
+        _check(lib().ssam_autotune_jacobi3d(n, nbatch, code, ctypes.c_void_p(stream.cuda_stream),
+                                            ctypes.byref(rep)))
     return rep.as_dict()
 
 

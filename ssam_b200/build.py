@@ -73,6 +73,50 @@ def instances():
     return out
 
 
+def instances_3d():
+    """(dtype, shape, r, PY, NW, S, rhs, default) of every compiled 3D
+    configuration: shape 0 = star (r = 1: 7-pt, r = 2: 13-pt), 1 = the
+    19-point Poisson operator; rhs = the Jacobi-sweep form with a
+    right-hand-side term.  The first of each group is the default; the 3D
+    autotuner times them all."""
+    cfg = {
+        "f32": {(0, 1): [(4, 8, 6), (4, 4, 8), (2, 16, 6), (4, 16, 5), (8, 8, 5)],
+                (0, 2): [(4, 4, 8), (4, 8, 6), (2, 8, 6), (2, 16, 6), (4, 12, 6)],
+                (1, 1): [(4, 8, 6), (4, 4, 8), (2, 16, 6), (4, 16, 5)],
+                "rhs": [(4, 8, 6), (4, 4, 8), (2, 16, 6), (4, 16, 5)]},
+        "bf16": {(0, 1): [(4, 8, 6), (2, 16, 6), (4, 16, 6), (8, 8, 6)],
+                 (0, 2): [(4, 4, 8), (4, 8, 6), (2, 16, 6)],
+                 (1, 1): [(4, 8, 6), (2, 16, 6), (4, 16, 6)],
+                 "rhs": [(4, 8, 6), (2, 16, 6), (4, 16, 6)]},
+        "f64": {(0, 1): [(4, 4, 5), (4, 8, 5), (2, 8, 5)],
+                (0, 2): [(4, 4, 6), (2, 8, 6)],
+                (1, 1): [(4, 4, 5), (2, 8, 5)],
+                "rhs": [(4, 4, 5), (2, 8, 5)]},
+        "f16": {(0, 1): [(4, 8, 6)], (0, 2): [(4, 4, 8)], (1, 1): [(4, 8, 6)]},
+    }
+    out = []
+    for dt, groups in cfg.items():
+        for key, lst in groups.items():
+            shape, r, rhs = (0, 1, True) if key == "rhs" else (key[0], key[1], False)
+            for i, (py, nw, s) in enumerate(lst):
+                out.append((dt, shape, r, py, nw, s, rhs, i == 0))
+    return out
+
+
+def stream_instances():
+    """(dtype, star, r, SEG, V) of every compiled row-streaming 2D kernel
+    (one step per launch; a warp walks SEG output rows), registered with
+    P = SEG: star r = 1..6 and box r = 1..5 at the default strip width."""
+    out = []
+    for dt in DTYPES:
+        v = 4 if dt in ("f32", "f64") else 8
+        for star, rmax in ((1, 6), (0, 5)):
+            for r in range(1, rmax + 1):
+                for seg in (32, 128):
+                    out.append((dt, star, r, seg, v))
+    return out
+
+
 def _gen_units(chunk: int = 6):
     os.makedirs(os.path.join(BUILD, "gen"), exist_ok=True)
     by_dt: dict[str, list] = {}
@@ -97,6 +141,49 @@ def _gen_units(chunk: int = 6):
                 with open(path, "w") as f:
                     f.write(text)
             units.append(path)
+    by_dt = {}
+    for inst in instances_3d():
+        by_dt.setdefault(inst[0], []).append(inst)
+    for dt, lst in by_dt.items():
+        for c in range(0, len(lst), 3):
+            part = lst[c:c + 3]
+            name = f"inst3d_{dt}_{c // 3:02d}.cu"
+            lines = ["// generated by ssam_b200/build.py -- do not edit",
+                     '#include "../../csrc/stencil3d_launch.cuh"', "namespace ssam {"]
+            for (_, shape, r, py, nw, s, rhs, dflt) in part:
+                sh = "SH3_POISSON19" if shape else "SH3_STAR"
+                tag = f"{shape}_{r}_{py}_{nw}_{s}_{int(rhs)}"
+                lines.append(
+                    f"static Register3D<{DTYPES[dt]}, {sh}, {r}, {py}, {nw}, {s}, "
+                    f"{'true' if rhs else 'false'}, {'true' if dflt else 'false'}> reg3_{tag};")
+            lines.append("}  // namespace ssam")
+            text = "\n".join(lines) + "\n"
+            path = os.path.join(BUILD, "gen", name)
+            if not os.path.exists(path) or open(path).read() != text:
+                with open(path, "w") as f:
+                    f.write(text)
+            units.append(path)
+    by_dt = {}
+    for inst in stream_instances():
+        by_dt.setdefault(inst[0], []).append(inst)
+    for dt, lst in by_dt.items():
+        for c in range(0, len(lst), chunk):
+            part = lst[c:c + chunk]
+            name = f"inst2ds_{dt}_{c // chunk:02d}.cu"
+            lines = ["// generated by ssam_b200/build.py -- do not edit",
+                     '#include "../../csrc/stencil2d_stream.cuh"', "namespace ssam {"]
+            for (_, star, r, seg, v) in part:
+                tag = f"{'s' if star else 'b'}_{r}_{seg}_{v}"
+                lines.append(
+                    f"static RegisterStream2D<{DTYPES[dt]}, {r}, {r}, {r}, {r}, "
+                    f"{'true' if star else 'false'}, {seg}, {v}> regs_{tag};")
+            lines.append("}  // namespace ssam")
+            text = "\n".join(lines) + "\n"
+            path = os.path.join(BUILD, "gen", name)
+            if not os.path.exists(path) or open(path).read() != text:
+                with open(path, "w") as f:
+                    f.write(text)
+            units.append(path)
     return units
 
 
@@ -107,13 +194,27 @@ def _nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
-def _headers_digest() -> str:
+def _local_headers(path: str, seen: set[str] | None = None) -> list[str]:
+    """The quoted #include files that `path` pulls in, recursively."""
+    seen = set() if seen is None else seen
+    with open(path) as f:
+        for line in f:
+            line = line.strip()
+            if line.startswith("#include") and '"' in line:
+                inc = os.path.normpath(os.path.join(os.path.dirname(path),
+                                                    line.split('"')[1]))
+                if inc not in seen and os.path.exists(inc):
+                    seen.add(inc)
+                    _local_headers(inc, seen)
+    return sorted(seen)
+
+
+def _unit_digest(src: str) -> str:
+    """Compiler flags plus the contents of the headers this unit includes."""
     h = hashlib.sha1()
-    for root in (CSRC, os.path.join(os.path.dirname(HERE), "include")):
-        for name in sorted(os.listdir(root)):
-            if name.endswith((".cuh", ".h")):
-                with open(os.path.join(root, name), "rb") as f:
-                    h.update(f.read())
+    for hdr in _local_headers(src):
+        with open(hdr, "rb") as f:
+            h.update(f.read())
     h.update(" ".join(NVFLAGS + ARCH).encode())
     return h.hexdigest()
 
@@ -140,13 +241,13 @@ def build(jobs: int | None = None, ptxas_verbose: bool = False, quiet: bool = Tr
     os.makedirs(BUILD, exist_ok=True)
     units = [os.path.join(CSRC, s) for s in SOURCES] + _gen_units()
     extra = ["-Xptxas", "-v"] if ptxas_verbose else []
-    stamp = _headers_digest() + ("v" if ptxas_verbose else "")
     jobs = jobs or max(1, os.cpu_count() or 1)
     objs = []
     with cf.ThreadPoolExecutor(jobs) as ex:
         futs = []
         for u in units:
             obj = os.path.join(BUILD, os.path.basename(u).replace(".cu", ".o"))
+            stamp = _unit_digest(u) + ("v" if ptxas_verbose else "")
             futs.append(ex.submit(_compile, u, obj, extra, stamp))
         for f in futs:
             objs.append(f.result())

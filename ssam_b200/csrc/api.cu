@@ -379,6 +379,30 @@ static int run_2d_host(const void* h_src, void* h_dst, int64_t w, int64_t h,
   return st;
 }
 
+// Argument checks shared by the 3D entry points and the 3D autotuner.
+int check_3d(const void* src, const void* dst, int64_t nx, int64_t ny, int64_t nz,
+             int dtype, int shape, int radius, const double* coeffs, int steps,
+             int boundary) {
+  if (!src || !dst) return fail(SSAM_ERR_INVALID, "src and dst must not be NULL");
+  if (nx < 1 || ny < 1 || nz < 1) return fail(SSAM_ERR_INVALID, "nx, ny, nz must be >= 1");
+  if (nx > (int64_t(1) << 31) || ny > (int64_t(1) << 31) || nz > (int64_t(1) << 31))
+    return fail(SSAM_ERR_INVALID, "grid side above 2^31");
+  if (!valid_dtype(dtype)) return fail(SSAM_ERR_INVALID, "unknown dtype");
+  if (shape != SSAM_STAR3D && shape != SSAM_POISSON19)
+    return fail(SSAM_ERR_INVALID, "shape must be SSAM_STAR3D or SSAM_POISSON19");
+  if (radius < 1 || radius > 4 || (shape == SSAM_POISSON19 && radius != 1))
+    return fail(SSAM_ERR_INVALID, "radius must be 1..4 (POISSON19: 1)");
+  if (!coeffs) return fail(SSAM_ERR_INVALID, "coeffs must not be NULL");
+  if (steps < 1) return fail(SSAM_ERR_INVALID, "steps must be >= 1");
+  if (boundary != SSAM_BOUNDARY_ZERO && boundary != SSAM_BOUNDARY_COPY)
+    return fail(boundary == SSAM_BOUNDARY_CLAMP ? SSAM_ERR_UNSUPPORTED : SSAM_ERR_INVALID,
+                "3D boundary must be ZERO or COPY");
+  const uintptr_t len = (uintptr_t)(nx * ny * nz) * dtype_size(dtype);
+  if ((uintptr_t)src < (uintptr_t)dst + len && (uintptr_t)dst < (uintptr_t)src + len)
+    return fail(SSAM_ERR_INVALID, "src and dst overlap (updates are out of place)");
+  return SSAM_OK;
+}
+
 }  // namespace ssam
 
 using namespace ssam;
@@ -424,29 +448,6 @@ int ssam_stencil2d_host(const void* h_src, void* h_dst, int64_t width, int64_t h
   return run_2d_host(h_src, h_dst, width, height, pitch, dtype, radius,
                      shape == SSAM_STAR ? 1 : 0, m.data(), steps, boundary,
                      (cudaStream_t)stream);
-}
-
-static int check_3d(const void* src, const void* dst, int64_t nx, int64_t ny, int64_t nz,
-                    int dtype, int shape, int radius, const double* coeffs, int steps,
-                    int boundary) {
-  if (!src || !dst) return fail(SSAM_ERR_INVALID, "src and dst must not be NULL");
-  if (nx < 1 || ny < 1 || nz < 1) return fail(SSAM_ERR_INVALID, "nx, ny, nz must be >= 1");
-  if (nx > (int64_t(1) << 31) || ny > (int64_t(1) << 31) || nz > (int64_t(1) << 31))
-    return fail(SSAM_ERR_INVALID, "grid side above 2^31");
-  if (!valid_dtype(dtype)) return fail(SSAM_ERR_INVALID, "unknown dtype");
-  if (shape != SSAM_STAR3D && shape != SSAM_POISSON19)
-    return fail(SSAM_ERR_INVALID, "shape must be SSAM_STAR3D or SSAM_POISSON19");
-  if (radius < 1 || radius > 4 || (shape == SSAM_POISSON19 && radius != 1))
-    return fail(SSAM_ERR_INVALID, "radius must be 1..4 (POISSON19: 1)");
-  if (!coeffs) return fail(SSAM_ERR_INVALID, "coeffs must not be NULL");
-  if (steps < 1) return fail(SSAM_ERR_INVALID, "steps must be >= 1");
-  if (boundary != SSAM_BOUNDARY_ZERO && boundary != SSAM_BOUNDARY_COPY)
-    return fail(boundary == SSAM_BOUNDARY_CLAMP ? SSAM_ERR_UNSUPPORTED : SSAM_ERR_INVALID,
-                "3D boundary must be ZERO or COPY");
-  const uintptr_t len = (uintptr_t)(nx * ny * nz) * dtype_size(dtype);
-  if ((uintptr_t)src < (uintptr_t)dst + len && (uintptr_t)dst < (uintptr_t)src + len)
-    return fail(SSAM_ERR_INVALID, "src and dst overlap (updates are out of place)");
-  return SSAM_OK;
 }
 
 int ssam_stencil3d(const void* src, void* dst, int64_t nx, int64_t ny, int64_t nz,

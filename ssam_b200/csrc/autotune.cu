@@ -267,6 +267,12 @@ extern "C" int ssam_autotune_save(const char* path) {
               std::get<8>(k), kv.second);
     }
   }
+  tune3d_for_each(
+      [](const int* k, const int* v, void* u) {
+        fprintf((FILE*)u, "choice3d %d %d %d %d %d %d %d %d %d %d\n", k[0], k[1], k[2], k[3],
+                k[4], k[5], k[6], v[0], v[1], v[2]);
+      },
+      f);
   fclose(f);
   return SSAM_OK;
 }
@@ -287,6 +293,10 @@ extern "C" int ssam_autotune_load(const char* path) {
       if (a[9] < 1 || a[10] < 1 || a[10] > 8 || a[11] < 1) { ++bad; continue; }
       c.choices[TuneKey{a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8]}] =
           TuneChoice{a[9], a[10], a[11]};
+    } else if (sscanf(line, "choice3d %d %d %d %d %d %d %d %d %d %d", &a[0], &a[1], &a[2],
+                      &a[3], &a[4], &a[5], &a[6], &a[7], &a[8], &a[9]) == 10) {
+      if (a[7] < 1 || a[8] < 1 || a[9] < 1) { ++bad; continue; }
+      tune3d_store(a, a + 7);
     } else if (sscanf(line, "depth %d %d %d %d %d %d %d %d %d", &a[0], &a[1], &a[2], &a[3],
                       &a[4], &a[5], &a[6], &a[7], &a[8]) == 9) {
       if (a[8] < 1) { ++bad; continue; }
@@ -301,9 +311,12 @@ extern "C" int ssam_autotune_load(const char* path) {
 }
 
 extern "C" int ssam_autotune_clear(void) {
-  TuneCache& c = cache();
-  std::lock_guard<std::mutex> g(c.mu);
-  c.choices.clear();
-  c.depths.clear();
+  {
+    TuneCache& c = cache();
+    std::lock_guard<std::mutex> g(c.mu);
+    c.choices.clear();
+    c.depths.clear();
+  }
+  tune3d_clear();
   return SSAM_OK;
 }

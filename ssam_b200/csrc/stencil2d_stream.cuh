@@ -1,0 +1,286 @@
+// Row-streaming variant of the register-cache systolic 2D kernel (one time
+// step per launch).
+//
+// The warp tile of stencil2d.cuh loads its whole window (P + rt + rb rows)
+// up front, computes P rows and stores them: the halo rows are read again by
+// the tile below, and a warp has loads in flight only between two compute
+// phases.  Here a warp walks SEG consecutive output rows of its 32*V-column
+// strip instead, keeping a ring of rows in registers:
+//   * the rows of the stencil's reach (rt + rb + 1 of them, converted to the
+//     accumulation type) plus D rows still in flight as raw 16-byte words;
+//   * every output row issues the load of the row D rows ahead of the reach,
+//     converts the row that has just come into reach, forms the row's sums
+//     with the same own-column / shuffled partial-sum scheme (SSAM's systolic
+//     exchange, reference ssai-2dstencil/stencil2D_*.cu), and stores it;
+//   * the ring is unrolled over its length, so every slot is a fixed set of
+//     registers (no local memory, no data movement between slots).
+// Each row of the strip is read once per segment (plus rt + rb + D rows at
+// the segment's ends), and every warp keeps D rows of loads in flight while it
+// computes.  Registered in the kernel table with P = SEG >= 32, which the
+// autotuner times against the windowed tiles.
+#pragma once
+
+#include "stencil2d.cuh"
+
+namespace ssam {
+
+template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int SEG, int V_>
+struct Stream2DCfg {
+  using TA = typename Traits<TS>::TA;
+  static constexpr int V = V_;
+  static constexpr int FW = RL + RR + 1;
+  static constexpr int FH = RT + RB + 1;
+  static constexpr int NC = FW * FH;
+  static constexpr int HL = (RL + V - 1) / V;  // halo lanes, left
+  static constexpr int HR = (RR + V - 1) / V;  // halo lanes, right
+  static constexpr int OUT_LANES = 32 - HL - HR;
+  static constexpr int OUT_COLS = OUT_LANES * V;
+  static constexpr int CH = V * (int)sizeof(TS) / 16;  // 16-byte words per row
+  // rows in flight ahead of the reach: 2 KB (FP32/16-bit) or 4 KB (FP64) a
+  // warp; one row for the 13-row reach, whose longer ring the compiler keeps
+  // in local memory
+  static constexpr int D = FH >= 13 ? 1 : 4;
+  static constexpr int L = FH + D;  // ring length = unroll factor
+  // rows a warp walks: SEG rounded up to whole ring lengths
+  static constexpr int SEGL = (SEG + L - 1) / L * L;
+  static_assert(OUT_LANES >= 2, "radius too large for one warp strip");
+  static_assert((V * sizeof(TS)) % 16 == 0, "a thread owns whole 16-byte chunks");
+};
+
+// Where a lane's V columns lie: all inside the grid, or (grids whose width is
+// a multiple of V, which the streaming kernel requires) all outside it, left
+// or right.
+enum StreamLane { kLaneIn = 0, kLaneLeft = 1, kLaneRight = 2 };
+
+template <typename TS, int V, int CH, typename TA>
+__device__ __forceinline__ void stream_unpack(TA (&d)[V], const uint4 (&w)[CH]) {
+  constexpr int PER = 16 / sizeof(TS);
+#pragma unroll
+  for (int c = 0; c < CH; ++c) {
+    const TS* e = reinterpret_cast<const TS*>(&w[c]);
+#pragma unroll
+    for (int k = 0; k < PER; ++k) d[c * PER + k] = to_acc(e[k]);
+  }
+}
+
+// Row y of the lane's (clamped) chunk as raw 16-byte words; rows outside the
+// grid are zero (ZERO) or the clamped edge row (CLAMP, COPY).
+template <typename TS, int CH>
+__device__ __forceinline__ void stream_load_row(uint4 (&w)[CH], const TS* __restrict__ src,
+                                                int64_t y, int64_t xc, int64_t H,
+                                                int64_t pitch, int bnd) {
+  const bool y_out = y < 0 || y >= H;
+  const uint4* row =
+      reinterpret_cast<const uint4*>(src + (y < 0 ? 0 : (y >= H ? H - 1 : y)) * pitch + xc);
+  if (y_out && bnd == SSAM_BOUNDARY_ZERO) {
+#pragma unroll
+    for (int c = 0; c < CH; ++c) w[c] = make_uint4(0u, 0u, 0u, 0u);
+  } else {
+#pragma unroll
+    for (int c = 0; c < CH; ++c) w[c] = __ldg(row + c);
+  }
+}
+
+// Values of an outside lane's columns after unpacking the (clamped) edge
+// chunk: 0 under ZERO, the edge column under CLAMP; under COPY they never
+// reach an output that is kept, so they stay as loaded.
+template <int V, typename TA>
+__device__ __forceinline__ void stream_fix_lane(TA (&d)[V], int where, int bnd) {
+  if (bnd == SSAM_BOUNDARY_ZERO) {
+#pragma unroll
+    for (int j = 0; j < V; ++j) d[j] = TA(0);
+  } else if (bnd == SSAM_BOUNDARY_CLAMP) {
+    const TA e = where == kLaneLeft ? d[0] : d[V - 1];
+#pragma unroll
+    for (int j = 0; j < V; ++j) d[j] = e;
+  }
+}
+
+// Requirements (checked by the launcher, which hands other grids to the
+// windowed kernel): src/dst 16-byte aligned, pitch and width multiples of V.
+// Then every lane's columns are a whole 16-byte-aligned chunk either inside
+// the grid or outside it, and all loads are 16-byte loads of a clamped chunk.
+template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int SEG, int V_>
+__global__ void __launch_bounds__(256)
+stencil2d_stream_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int64_t W,
+                        int64_t H, int64_t pitch, int64_t y_begin, int64_t y_end, int bnd,
+                        CoefBlock<typename Traits<TS>::TA,
+                                  Stream2DCfg<TS, RL, RR, RT, RB, STAR, SEG, V_>::NC> cf) {
+  using C = Stream2DCfg<TS, RL, RR, RT, RB, STAR, SEG, V_>;
+  using TA = typename C::TA;
+  constexpr int V = C::V, FW = C::FW, FH = C::FH, CH = C::CH, D = C::D, L = C::L;
+  constexpr int SEGL = C::SEGL;
+  constexpr unsigned FULL = 0xffffffffu;
+  const int64_t warp_x = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int64_t x_out0 = warp_x * C::OUT_COLS;
+  if (x_out0 >= W) return;  // whole warp leaves together
+  const int lane = threadIdx.x & 31;
+  const int64_t x0 = x_out0 + (int64_t)(lane - C::HL) * V;
+  const bool lane_stores = lane >= C::HL && lane < 32 - C::HR && x0 < W;
+  const int where = x0 < 0 ? kLaneLeft : (x0 >= W ? kLaneRight : kLaneIn);
+  // this lane's chunk, clamped into the grid
+  const int64_t xc = x0 < 0 ? 0 : (x0 >= W ? W - V : x0);
+  // warp-uniform: some lane of this warp lies outside the grid
+  const bool edge_warp = x_out0 - (int64_t)C::HL * V < 0 || x_out0 + (32 - C::HL) * V > W;
+  // columns of this lane that the COPY rule keeps at their input value
+  const bool x_copy = bnd == SSAM_BOUNDARY_COPY && (x0 < RL || x0 + V > W - RR);
+  const int64_t nseg = (y_end - y_begin + SEGL - 1) / SEGL;
+
+  for (int64_t sg = blockIdx.y; sg < nseg; sg += gridDim.y) {
+    const int64_t ya = y_begin + sg * SEGL;  // first output row of the segment
+    // ring slot of grid row ya + k (k >= -RT) is (k + RT) % L
+    uint4 raw[L][CH];
+    TA val[L][V];
+    // prologue: rows ya-RT .. ya+RB+D-1 in flight, ya-RT .. ya+RB-1 converted
+#pragma unroll
+    for (int k = 0; k < FH - 1 + D; ++k) stream_load_row<TS, CH>(raw[k], src, ya - RT + k, xc, H, pitch, bnd);
+#pragma unroll
+    for (int k = 0; k < FH - 1; ++k) {
+      stream_unpack<TS, V, CH>(val[k], raw[k]);
+      if (edge_warp && where != kLaneIn) stream_fix_lane<V>(val[k], where, bnd);
+    }
+
+    // whole groups of L rows (rows past y_end are computed, not stored)
+    const int64_t left = y_end - ya;
+    const int nrows = left < SEGL ? (int)left : SEGL;
+    for (int base = 0; base < nrows; base += L) {
+#pragma unroll
+      for (int u = 0; u < L; ++u) {
+        const int i = base + u;  // output row ya + i
+        // the row D ahead of the reach; its slot held row ya+i-RT-1, now done
+        stream_load_row<TS, CH>(raw[(u + FH - 1 + D) % L], src, ya + i + RB + D, xc, H,
+                                pitch, bnd);
+        // the row entering the reach
+        stream_unpack<TS, V, CH>(val[(u + FH - 1) % L], raw[(u + FH - 1) % L]);
+        if (edge_warp && where != kLaneIn)
+          stream_fix_lane<V>(val[(u + FH - 1) % L], where, bnd);
+
+        TA acc[V];
+#pragma unroll
+        for (int j = 0; j < V; ++j) acc[j] = TA(0);
+        // own columns
+#pragma unroll
+        for (int dy = -RT; dy <= RB; ++dy) {
+#pragma unroll
+          for (int dx = -RL; dx <= RR; ++dx) {
+            if (STAR && dy != 0 && dx != 0) continue;
+            const TA w = cf.c[(dy + RT) * FW + (dx + RL)];
+#pragma unroll
+            for (int j = 0; j < V; ++j) {
+              if (j + dx < 0 || j + dx >= V) continue;
+              acc[j] = fma(w, val[(u + RT + dy) % L][j + dx], acc[j]);
+            }
+          }
+        }
+        // partial sums travelling right: virtual column V+q, q < RL
+        if constexpr (RL > 0) {
+          TA pr[RL];
+#pragma unroll
+          for (int q = 0; q < RL; ++q) {
+            pr[q] = TA(0);
+#pragma unroll
+            for (int dy = -RT; dy <= RB; ++dy) {
+              if (STAR && dy != 0) continue;
+#pragma unroll
+              for (int j = 0; j < V; ++j) {
+                const int dx = j - V - q;
+                if (dx < -RL || dx > -1) continue;
+                pr[q] = fma(cf.c[(dy + RT) * FW + (dx + RL)], val[(u + RT + dy) % L][j],
+                            pr[q]);
+              }
+            }
+          }
+          constexpr int K = (RL + V - 1) / V;
+#pragma unroll
+          for (int st = K - 1; st >= 0; --st) {
+#pragma unroll
+            for (int q = st * V; q < (st + 1) * V && q < RL; ++q) {
+              const TA v = __shfl_up_sync(FULL, pr[q], 1);
+              if (st == 0) acc[q] += v;
+              else pr[q - V] += v;
+            }
+          }
+        }
+        // partial sums travelling left: virtual column -1-q, q < RR
+        if constexpr (RR > 0) {
+          TA pl[RR];
+#pragma unroll
+          for (int q = 0; q < RR; ++q) {
+            pl[q] = TA(0);
+#pragma unroll
+            for (int dy = -RT; dy <= RB; ++dy) {
+              if (STAR && dy != 0) continue;
+#pragma unroll
+              for (int j = 0; j < V; ++j) {
+                const int dx = j + 1 + q;
+                if (dx < 1 || dx > RR) continue;
+                pl[q] = fma(cf.c[(dy + RT) * FW + (dx + RL)], val[(u + RT + dy) % L][j],
+                            pl[q]);
+              }
+            }
+          }
+          constexpr int K = (RR + V - 1) / V;
+#pragma unroll
+          for (int st = K - 1; st >= 0; --st) {
+#pragma unroll
+            for (int q = st * V; q < (st + 1) * V && q < RR; ++q) {
+              const TA v = __shfl_down_sync(FULL, pl[q], 1);
+              if (st == 0) acc[V - 1 - q] += v;
+              else pl[q - V] += v;
+            }
+          }
+        }
+        const int64_t y = ya + i;
+        if (bnd == SSAM_BOUNDARY_COPY && (x_copy || y < RT || y >= H - RB)) {
+#pragma unroll
+          for (int j = 0; j < V; ++j) {
+            const int64_t x = x0 + j;
+            if ((x < RL) | (x >= W - RR) | (y < RT) | (y >= H - RB))
+              acc[j] = val[(u + RT) % L][j];
+          }
+        }
+        if (lane_stores && y < y_end) store_vec<TS, V>(dst + y * pitch + x0, acc);
+      }
+    }
+  }
+}
+
+template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int SEG, int V_>
+cudaError_t launch_stencil2d_stream(const Launch2D& a) {
+  using C = Stream2DCfg<TS, RL, RR, RT, RB, STAR, SEG, V_>;
+  using TA = typename C::TA;
+  CoefBlock<TA, C::NC> cf;
+  for (int k = 0; k < C::NC; ++k) cf.c[k] = (TA)a.coef[k];
+  const int nw = a.warps_per_block;
+  const int64_t warps_x = (a.width + C::OUT_COLS - 1) / C::OUT_COLS;
+  const int64_t nseg = (a.y_end - a.y_begin + C::SEGL - 1) / C::SEGL;
+  dim3 grid((unsigned)((warps_x + nw - 1) / nw), (unsigned)(nseg < 65535 ? nseg : 65535));
+  const bool aligned = ((uintptr_t)a.src % 16 == 0) && ((uintptr_t)a.dst % 16 == 0) &&
+                       (a.pitch % C::V == 0) && (a.width % C::V == 0);
+  if (!aligned) {
+    // unaligned grids: the windowed kernel of the same stencil
+    const Kernel2DInfo* w =
+        find_2d(Key2D{Traits<TS>::DT, RL, RR, RT, RB, STAR ? 1 : 0, 8, 1, V_});
+    if (!w) return cudaErrorInvalidValue;
+    return w->launch(a);
+  }
+  stencil2d_stream_kernel<TS, RL, RR, RT, RB, STAR, SEG, V_><<<grid, 32 * nw, 0, a.stream>>>(
+      (const TS*)a.src, (TS*)a.dst, a.width, a.height, a.pitch, a.y_begin, a.y_end,
+      a.boundary, cf);
+  count_launch();
+  return cudaGetLastError();
+}
+
+template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int SEG, int V_>
+struct RegisterStream2D {
+  static_assert(SEG >= 32, "P >= 32 marks a streaming kernel in the table");
+  RegisterStream2D() {
+    Kernel2DInfo info;
+    info.launch = &launch_stencil2d_stream<TS, RL, RR, RT, RB, STAR, SEG, V_>;
+    info.func = (const void*)&stencil2d_stream_kernel<TS, RL, RR, RT, RB, STAR, SEG, V_>;
+    info.vec = V_;
+    register_2d(Key2D{Traits<TS>::DT, RL, RR, RT, RB, STAR ? 1 : 0, SEG, 1, V_}, info);
+  }
+};
+
+}  // namespace ssam

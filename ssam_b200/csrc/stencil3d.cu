@@ -1,6 +1,8 @@
-// Host side of the 3D stencils: tensor maps, persistent work split, the
-// compiled (dtype, shape, radius) set, multi-step chaining and CUDA-graph
-// capture of timestep loops.
+// Host side of the 3D stencils: the table of compiled configurations, the
+// measured choice per grid size (ssam_autotune_stencil3d), multi-step
+// chaining and CUDA-graph capture of timestep loops.  The launcher template
+// is in stencil3d_launch.cuh; the configurations are instantiated in
+// generated units (ssam_b200/build.py).
 #include <cudaTypedefs.h>
 #include <string.h>
 
@@ -10,7 +12,8 @@
 #include <tuple>
 #include <vector>
 
-#include "stencil3d.cuh"
+#include "autotune.h"
+#include "stencil3d_launch.cuh"
 
 namespace ssam {
 
@@ -50,156 +53,89 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 // driver does not provide it).
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() { return encode_fn(); }
 
-template <typename TS> CUtensorMapDataType tma_dtype();
-template <> CUtensorMapDataType tma_dtype<float>() { return CU_TENSOR_MAP_DATA_TYPE_FLOAT32; }
-template <> CUtensorMapDataType tma_dtype<double>() { return CU_TENSOR_MAP_DATA_TYPE_FLOAT64; }
-template <> CUtensorMapDataType tma_dtype<__nv_bfloat16>() {
-  return CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+
+// ------------------------------------------------- configuration table --
+
+using Key3D = std::tuple<int, int, int, int>;  // dtype, shape, radius, rhs
+
+static std::map<Key3D, std::vector<Cand3D>>& table_3d() {
+  static std::map<Key3D, std::vector<Cand3D>> t;
+  return t;
 }
-template <> CUtensorMapDataType tma_dtype<__half>() { return CU_TENSOR_MAP_DATA_TYPE_FLOAT16; }
 
-struct Launch3D {
-  const void* src;
-  void* dst;
-  int64_t nx, ny, nz;
-  int nb;              // grids stacked along a 4th axis (1 = plain 3D grid)
-  const void* rhs;     // NULL, or out += rhs_scale * rhs
-  double rhs_scale;
-  const double* coef;  // (2R+1)^3, [dz][dy][dx]
-  int boundary;
-  cudaStream_t stream;
-  bool prepare_only;  // resolve attributes/occupancy/symbols, launch nothing
-};
+void register_3d(int dtype, int shape, int r, bool rhs, const Cand3D& c) {
+  table_3d()[Key3D{dtype, shape, r, rhs ? 1 : 0}].push_back(c);
+}
 
-template <typename TS, int SH, int R, int PY, int NW, int S, bool RHS = false>
-static int launch_3d(const Launch3D& a) {
-  using C = Stencil3DCfg<TS, SH, R, PY, NW, S>;
-  using TA = typename C::TA;
-  auto kern = stencil3d_kernel<TS, SH, R, PY, NW, S, RHS>;
-  if ((a.rhs != nullptr) != RHS)
-    return fail(SSAM_ERR_INVALID, "3D kernel instance does not match the right-hand side");
-  static std::mutex mu;
-  static std::map<int, int> ctas_per_sm;  // per device
-  int dev = 0;
-  SSAM_CUDA_TRY(cudaGetDevice(&dev));
-  int bps, sms;
+static const std::vector<Cand3D>* cands_3d(int dtype, int shape, int r, bool rhs) {
+  auto it = table_3d().find(Key3D{dtype, shape, r, rhs ? 1 : 0});
+  return it == table_3d().end() || it->second.empty() ? nullptr : &it->second;
+}
+
+// Measured choices: (dtype, shape, radius, rhs, log2 nx, log2 ny, log2 nz*nb)
+// -> (PY, NW, S).
+using Tune3DKey = std::tuple<int, int, int, int, int, int, int>;
+static std::mutex g_tune3_mu;
+static std::map<Tune3DKey, std::tuple<int, int, int>> g_tune3;
+
+static int log2_floor(int64_t v) {
+  int b = 0;
+  while (v > 1) {
+    v >>= 1;
+    ++b;
+  }
+  return b;
+}
+
+static Tune3DKey tune3_key(int dtype, int shape, int r, bool rhs, int64_t nx, int64_t ny,
+                           int64_t nzb) {
+  return Tune3DKey{dtype, shape, r, rhs ? 1 : 0, log2_floor(nx), log2_floor(ny),
+                   log2_floor(nzb)};
+}
+
+// The configuration for one launch: the measured one for this size class if
+// any, else the default.
+static const Cand3D* pick_3d(int dtype, int shape, int r, bool rhs, int64_t nx, int64_t ny,
+                             int64_t nzb) {
+  const std::vector<Cand3D>* cs = cands_3d(dtype, shape, r, rhs);
+  if (!cs) return nullptr;
   {
-    std::lock_guard<std::mutex> g(mu);
-    auto it = ctas_per_sm.find(dev);
-    if (it == ctas_per_sm.end()) {
-      SSAM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         C::SMEM));
-      int b = 0;
-      SSAM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, C::THREADS,
-                                                                  C::SMEM));
-      if (b < 1) return fail(SSAM_ERR_UNSUPPORTED, "3D kernel does not fit on an SM");
-      it = ctas_per_sm.emplace(dev, b).first;
-    }
-    bps = it->second;
+    std::lock_guard<std::mutex> g(g_tune3_mu);
+    auto it = g_tune3.find(tune3_key(dtype, shape, r, rhs, nx, ny, nzb));
+    if (it != g_tune3.end())
+      for (const Cand3D& c : *cs)
+        if (std::make_tuple(c.py, c.nw, c.s) == it->second) return &c;
   }
-  SSAM_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-
-  const size_t es = sizeof(TS);
-  Work3D w;
-  w.nx = a.nx;
-  w.ny = a.ny;
-  w.nz = a.nz;
-  w.nb = a.nb;
-  w.rhs = a.rhs;
-  w.rhs_scale = a.rhs_scale;
-  w.ntx = (int)((a.nx + C::TX - 1) / C::TX);
-  w.nty = (int)((a.ny + C::TY - 1) / C::TY);
-  // z chunk: minimise (rounds of items) x (chunk + 2R prologue planes)
-  const int64_t grid_max = (int64_t)sms * bps;
-  const int64_t ntiles = (int64_t)w.ntx * w.nty;
-  int64_t best = -1;
-  for (int zc : {8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512}) {
-    if (zc > 2 * a.nz && zc > 8) break;
-    const int64_t items = ntiles * ((a.nz + zc - 1) / zc) * a.nb;
-    const int64_t rounds = (items + grid_max - 1) / grid_max;
-    const int64_t cost = rounds * (std::min<int64_t>(zc, a.nz) + 2 * R);
-    if (best < 0 || cost < best) {
-      best = cost;
-      w.zc = zc;
-      w.items = items;
-    }
-  }
-  const int64_t grid = std::min(w.items, grid_max);
-  w.boundary = a.boundary;
-  w.wait_ns = 1000ull * 1000ull * 1000ull;  // 1 s per wait; healthy waits take microseconds
-  int st = device_error_word(&w.err);
-  if (st != SSAM_OK) return st;
-  if (a.prepare_only) return SSAM_OK;
-
-  CUtensorMap map;
-  memset(&map, 0, sizeof(map));
-  w.use_tma = ((uintptr_t)a.src % 16 == 0) && ((a.nx * (int64_t)es) % 16 == 0) &&
-              a.nx <= (int64_t(1) << 32) && encode_fn() != nullptr;
-  if (w.use_tma) {
-    cuuint64_t dims[4] = {(cuuint64_t)a.nx, (cuuint64_t)a.ny, (cuuint64_t)a.nz,
-                          (cuuint64_t)a.nb};
-    cuuint64_t strides[3] = {(cuuint64_t)(a.nx * es), (cuuint64_t)(a.nx * a.ny * es),
-                             (cuuint64_t)(a.nx * a.ny * a.nz * es)};
-    cuuint32_t box[4] = {(cuuint32_t)C::XW, (cuuint32_t)C::YW, 1, 1};
-    cuuint32_t estr[4] = {1, 1, 1, 1};
-    CUresult r = encode_fn()(&map, tma_dtype<TS>(), 4, const_cast<void*>(a.src), dims,
-                             strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) w.use_tma = 0;  // fall back to plain loads
-  }
-  CoefBlock<TA, C::NC> cf;
-  for (int k = 0; k < C::NC; ++k) cf.c[k] = (TA)a.coef[k];
-  kern<<<(unsigned)grid, C::THREADS, C::SMEM, a.stream>>>(map, (const TS*)a.src, (TS*)a.dst,
-                                                          w, cf);
-  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-  cudaStreamIsCapturing(a.stream, &cap);
-  if (cap == cudaStreamCaptureStatusNone) count_launch();  // graphs count at replay
-  SSAM_CUDA_TRY(cudaGetLastError());
-  return SSAM_OK;
+  for (const Cand3D& c : *cs)
+    if (c.dflt) return &c;
+  return &cs->front();
 }
 
-using LaunchFn3D = int (*)(const Launch3D&);
-
-// (dtype, shape, radius) -> kernel.  Tile heights and ring depths keep the
-// shared-memory ring at <= ~113 KB so that two CTAs fit on an SM.
-static LaunchFn3D find_3d(int dtype, int shape, int r) {
-  if (shape == SH3_STAR && r == 1) {
-    switch (dtype) {
-      case SSAM_F32: return &launch_3d<float, SH3_STAR, 1, 4, 8, 6>;
-      case SSAM_F64: return &launch_3d<double, SH3_STAR, 1, 4, 4, 5>;
-      case SSAM_BF16: return &launch_3d<__nv_bfloat16, SH3_STAR, 1, 4, 8, 6>;
-      case SSAM_F16: return &launch_3d<__half, SH3_STAR, 1, 4, 8, 6>;
-    }
+void tune3d_for_each(void (*cb)(const int key[7], const int val[3], void*), void* user) {
+  std::lock_guard<std::mutex> g(g_tune3_mu);
+  for (auto& kv : g_tune3) {
+    const int k[7] = {std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first),
+                      std::get<3>(kv.first), std::get<4>(kv.first), std::get<5>(kv.first),
+                      std::get<6>(kv.first)};
+    const int v[3] = {std::get<0>(kv.second), std::get<1>(kv.second), std::get<2>(kv.second)};
+    cb(k, v, user);
   }
-  if (shape == SH3_STAR && r == 2) {
-    switch (dtype) {
-      case SSAM_F32: return &launch_3d<float, SH3_STAR, 2, 4, 4, 8>;
-      case SSAM_F64: return &launch_3d<double, SH3_STAR, 2, 4, 4, 6>;
-      case SSAM_BF16: return &launch_3d<__nv_bfloat16, SH3_STAR, 2, 4, 4, 8>;
-      case SSAM_F16: return &launch_3d<__half, SH3_STAR, 2, 4, 4, 8>;
-    }
-  }
-  if (shape == SH3_POISSON19 && r == 1) {
-    switch (dtype) {
-      case SSAM_F32: return &launch_3d<float, SH3_POISSON19, 1, 4, 8, 6>;
-      case SSAM_F64: return &launch_3d<double, SH3_POISSON19, 1, 4, 4, 5>;
-      case SSAM_BF16: return &launch_3d<__nv_bfloat16, SH3_POISSON19, 1, 4, 8, 6>;
-      case SSAM_F16: return &launch_3d<__half, SH3_POISSON19, 1, 4, 8, 6>;
-    }
-  }
-  return nullptr;
 }
 
-// The 7-point instances with the right-hand-side term (the Jacobi sweep).
-static LaunchFn3D find_3d_rhs(int dtype) {
-  switch (dtype) {
-    case SSAM_F32: return &launch_3d<float, SH3_STAR, 1, 4, 8, 6, true>;
-    case SSAM_F64: return &launch_3d<double, SH3_STAR, 1, 4, 4, 5, true>;
-    case SSAM_BF16: return &launch_3d<__nv_bfloat16, SH3_STAR, 1, 4, 8, 6, true>;
-  }
-  return nullptr;
+void tune3d_store(const int key[7], const int val[3]) {
+  std::lock_guard<std::mutex> g(g_tune3_mu);
+  g_tune3[Tune3DKey{key[0], key[1], key[2], key[3], key[4], key[5], key[6]}] =
+      std::make_tuple(val[0], val[1], val[2]);
 }
+
+void tune3d_clear() {
+  std::lock_guard<std::mutex> g(g_tune3_mu);
+  g_tune3.clear();
+}
+
+static const char* kNo3D =
+    "no 3D kernel for this dtype/shape/radius (have: star r=1 (7-pt), star r=2 (13-pt), "
+    "poisson19)";
 
 // ------------------------------------------------------ multi-step + graphs --
 
@@ -209,10 +145,11 @@ struct GraphKey {
   int64_t nx, ny, nz;
   int dtype, shape, r, steps, boundary;
   std::vector<double> coef;
+  LaunchFn3D fn;  // the configuration captured (a new measured choice recaptures)
   bool operator<(const GraphKey& o) const {
-    return std::tie(src, dst, nx, ny, nz, dtype, shape, r, steps, boundary, coef) <
+    return std::tie(src, dst, nx, ny, nz, dtype, shape, r, steps, boundary, coef, fn) <
            std::tie(o.src, o.dst, o.nx, o.ny, o.nz, o.dtype, o.shape, o.r, o.steps,
-                    o.boundary, o.coef);
+                    o.boundary, o.coef, o.fn);
   }
 };
 
@@ -264,13 +201,12 @@ static int enqueue_chain_3d(LaunchFn3D fn, const GraphKey& k, void* scratch,
 int run_3d(const void* src, void* dst, int64_t nx, int64_t ny, int64_t nz, int dtype,
            int shape, int r, const double* coef, int steps, int boundary, int use_graph,
            cudaStream_t stream) {
-  LaunchFn3D fn = find_3d(dtype, shape, r);
-  if (!fn)
-    return fail(SSAM_ERR_UNSUPPORTED, "no 3D kernel for this dtype/shape/radius (have: "
-                                      "star r=1 (7-pt), star r=2 (13-pt), poisson19)");
+  const Cand3D* c = pick_3d(dtype, shape, r, false, nx, ny, nz);
+  if (!c) return fail(SSAM_ERR_UNSUPPORTED, kNo3D);
+  LaunchFn3D fn = c->fn;
   const int f = 2 * r + 1;
   GraphKey k{src, dst, nx, ny, nz, dtype, shape, r, steps, boundary,
-             std::vector<double>(coef, coef + f * f * f)};
+             std::vector<double>(coef, coef + f * f * f), fn};
   if (steps == 1) return enqueue_chain_3d(fn, k, nullptr, stream);
 
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
@@ -359,10 +295,144 @@ namespace ssam {
 // (Dirichlet) boundary.  Used by the Poisson Jacobi sweeps.
 int sweep_3d(const void* in, void* out, int64_t n, int nb, int dtype, const double* cube,
              const void* rhs, double rhs_scale, cudaStream_t s) {
-  LaunchFn3D fn = rhs ? find_3d_rhs(dtype) : find_3d(dtype, SH3_STAR, 1);
-  if (!fn) return fail(SSAM_ERR_UNSUPPORTED, "no 3D 7-point kernel for this dtype");
+  const Cand3D* c = pick_3d(dtype, SH3_STAR, 1, rhs != nullptr, n, n, n * nb);
+  if (!c) return fail(SSAM_ERR_UNSUPPORTED, "no 3D 7-point kernel for this dtype");
   Launch3D a{in, out, n, n, n, nb, rhs, rhs_scale, cube, SSAM_BOUNDARY_ZERO, s, false};
-  return fn(a);
+  return c->fn(a);
 }
 
 }  // namespace ssam
+
+// ------------------------------------------------------------ autotuner --
+
+namespace ssam {
+
+int check_3d(const void* src, const void* dst, int64_t nx, int64_t ny, int64_t nz,
+             int dtype, int shape, int radius, const double* coeffs, int steps,
+             int boundary);
+
+// Mean time (ms) of one launch of `c`, after one untimed launch; repetitions
+// cover about 3 ms.
+static int time_3d(const Cand3D& c, const Launch3D& a, cudaEvent_t e0, cudaEvent_t e1,
+                   double* ms_out) {
+  int st = c.fn(a);
+  if (st != SSAM_OK) return st;
+  SSAM_CUDA_TRY(cudaEventRecord(e0, a.stream));
+  st = c.fn(a);
+  if (st != SSAM_OK) return st;
+  SSAM_CUDA_TRY(cudaEventRecord(e1, a.stream));
+  SSAM_CUDA_TRY(cudaEventSynchronize(e1));
+  float one = 0.f;
+  SSAM_CUDA_TRY(cudaEventElapsedTime(&one, e0, e1));
+  int reps = one > 0.f ? (int)(3.0f / one) : 20;
+  reps = reps < 2 ? 2 : (reps > 20 ? 20 : reps);
+  SSAM_CUDA_TRY(cudaEventRecord(e0, a.stream));
+  for (int i = 0; i < reps; ++i) {
+    st = c.fn(a);
+    if (st != SSAM_OK) return st;
+  }
+  SSAM_CUDA_TRY(cudaEventRecord(e1, a.stream));
+  SSAM_CUDA_TRY(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  SSAM_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+  *ms_out = ms / reps;
+  return SSAM_OK;
+}
+
+// Times every configuration in `cs` with launch `a` (its fn ignored) and
+// stores the fastest under `key`.
+static int tune_3d(const std::vector<Cand3D>& cs, const Launch3D& a, const Tune3DKey& key,
+                   ssam_tune3d_report* report) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  SSAM_CUDA_TRY(cudaEventCreate(&e0));
+  cudaError_t ce = cudaEventCreate(&e1);
+  if (ce != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return fail_cuda(ce, "cudaEventCreate");
+  }
+  int st = SSAM_OK, timed = 0;
+  const Cand3D* best = nullptr;
+  double best_ms = 0;
+  for (const Cand3D& c : cs) {
+    double ms = 0;
+    st = time_3d(c, a, e0, e1, &ms);
+    if (st != SSAM_OK) break;
+    ++timed;
+    if (!best || ms < best_ms) {
+      best = &c;
+      best_ms = ms;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != SSAM_OK) return st;
+  int* err = nullptr;
+  st = device_error_word(&err);
+  if (st != SSAM_OK) return st;
+  int code = 0;
+  SSAM_CUDA_TRY(cudaMemcpy(&code, err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (code != 0)
+    return fail(SSAM_ERR_TIMEOUT, "a 3D kernel gave up waiting while being timed (code " +
+                                     std::to_string(code) + ")");
+  {
+    std::lock_guard<std::mutex> g(g_tune3_mu);
+    g_tune3[key] = std::make_tuple(best->py, best->nw, best->s);
+  }
+  if (report) {
+    report->rows_per_warp = best->py;
+    report->consumer_warps = best->nw;
+    report->ring_slots = best->s;
+    report->candidates = timed;
+    report->ms_per_step = best_ms;
+  }
+  return SSAM_OK;
+}
+
+}  // namespace ssam
+
+using namespace ssam;
+
+extern "C" int ssam_autotune_stencil3d(const void* src, void* dst, int64_t nx, int64_t ny,
+                                       int64_t nz, int dtype, int shape, int radius,
+                                       const double* coeffs, int boundary, void* stream,
+                                       ssam_tune3d_report* report) {
+  int st = check_3d(src, dst, nx, ny, nz, dtype, shape, radius, coeffs, 1, boundary);
+  if (st != SSAM_OK) return st;
+  const int sh = shape == SSAM_POISSON19 ? SH3_POISSON19 : SH3_STAR;
+  const std::vector<Cand3D>* cs = cands_3d(dtype, sh, radius, false);
+  if (!cs) return fail(SSAM_ERR_UNSUPPORTED, kNo3D);
+  Launch3D a{src, dst, nx, ny, nz, 1, nullptr, 0.0, coeffs, boundary, (cudaStream_t)stream,
+             false};
+  return tune_3d(*cs, a, tune3_key(dtype, sh, radius, false, nx, ny, nz), report);
+}
+
+extern "C" int ssam_autotune_jacobi3d(int64_t n, int nbatch, int sweep_dtype, void* stream,
+                                      ssam_tune3d_report* report) {
+  if (n < 1 || nbatch < 1) return fail(SSAM_ERR_INVALID, "n and nbatch must be >= 1");
+  if (n > 4096) return fail(SSAM_ERR_INVALID, "n above 4096");
+  if (sweep_dtype != SSAM_F32 && sweep_dtype != SSAM_BF16)
+    return fail(SSAM_ERR_INVALID, "sweep_dtype must be SSAM_F32 or SSAM_BF16");
+  const std::vector<Cand3D>* cs = cands_3d(sweep_dtype, SH3_STAR, 1, true);
+  if (!cs) return fail(SSAM_ERR_UNSUPPORTED, "no Jacobi sweep kernel for this dtype");
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t bytes = (size_t)(n * n * n) * (size_t)nbatch * dtype_size(sweep_dtype);
+  void* buf[3] = {nullptr, nullptr, nullptr};
+  int st = SSAM_OK;
+  for (int i = 0; i < 3 && st == SSAM_OK; ++i) {
+    st = scratch_alloc(&buf[i], bytes, s);
+    if (st == SSAM_OK) {
+      cudaError_t e = cudaMemsetAsync(buf[i], 0, bytes, s);
+      if (e != cudaSuccess) st = fail_cuda(e, "cudaMemsetAsync");
+    }
+  }
+  if (st == SSAM_OK) {
+    // the sweep's operator: centre 0, neighbours 1/6 (values do not change the time)
+    double cube[27] = {0};
+    for (int k : {4, 10, 12, 14, 16, 22}) cube[k] = 1.0 / 6.0;
+    Launch3D a{buf[0], buf[1], n, n, n, nbatch, buf[2], 1.0 / 6.0, cube, SSAM_BOUNDARY_ZERO,
+               s, false};
+    st = tune_3d(*cs, a, tune3_key(sweep_dtype, SH3_STAR, 1, true, n, n, n * nbatch), report);
+  }
+  for (int i = 0; i < 3; ++i) scratch_free(buf[i], s);
+  return st;
+}

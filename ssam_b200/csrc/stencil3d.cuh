@@ -79,6 +79,9 @@ struct Stencil3DCfg {
   static constexpr int SMEM = S * SLOT_BYTES + 2 * S * 8 + 128;
   static constexpr int NC = (2 * R + 1) * (2 * R + 1) * (2 * R + 1);
   static constexpr int THREADS = 32 * (NW + 1);
+  // CTAs per SM the register budget is cut for: two when two rings fit in
+  // shared memory and the CTA is at most 9 warps, else one
+  static constexpr int MINB = (NW < 12 && 2 * (SMEM + 1024) <= 233472) ? 2 : 1;
   static_assert(R <= HX && R <= V, "x reach must fit in the halo and one lane hop");
   static_assert(S >= 2 * R + 2, "ring must hold the stencil window plus one plane");
 };
@@ -218,7 +221,7 @@ __device__ __forceinline__ Seg3D item_seg(int64_t it, const Work3D& w) {
 // loaded at the top of every plane, so their latency overlaps the plane's
 // barrier waits and arithmetic (instances without it carry no rhs code).
 template <typename TS, int SH, int R, int PY, int NW, int S, bool RHS = false>
-__global__ void __launch_bounds__(32 * (NW + 1), 2)
+__global__ void __launch_bounds__(32 * (NW + 1), (Stencil3DCfg<TS, SH, R, PY, NW, S>::MINB))
 stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__ src,
                  TS* __restrict__ dst, Work3D w,
                  CoefBlock<typename Traits<TS>::TA,

@@ -1,0 +1,158 @@
+// Host-side launcher of the 3D z-marching kernel, one template instance per
+// compiled configuration, and the registrar through which the generated
+// instantiation units add configurations to the library's 3D table.
+#pragma once
+
+#include <cudaTypedefs.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <mutex>
+
+#include "stencil3d.cuh"
+
+namespace ssam {
+
+// The driver's tensor-map encoder (NULL if the driver does not provide it).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
+
+template <typename TS> CUtensorMapDataType tma_dtype();
+template <> inline CUtensorMapDataType tma_dtype<float>() {
+  return CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+}
+template <> inline CUtensorMapDataType tma_dtype<double>() {
+  return CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+}
+template <> inline CUtensorMapDataType tma_dtype<__nv_bfloat16>() {
+  return CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+}
+template <> inline CUtensorMapDataType tma_dtype<__half>() {
+  return CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+}
+
+struct Launch3D {
+  const void* src;
+  void* dst;
+  int64_t nx, ny, nz;
+  int nb;              // grids stacked along a 4th axis (1 = plain 3D grid)
+  const void* rhs;     // NULL, or out += rhs_scale * rhs
+  double rhs_scale;
+  const double* coef;  // (2R+1)^3, [dz][dy][dx]
+  int boundary;
+  cudaStream_t stream;
+  bool prepare_only;  // resolve attributes/occupancy/symbols, launch nothing
+};
+
+template <typename TS, int SH, int R, int PY, int NW, int S, bool RHS = false>
+int launch_3d(const Launch3D& a) {
+  using C = Stencil3DCfg<TS, SH, R, PY, NW, S>;
+  using TA = typename C::TA;
+  auto kern = stencil3d_kernel<TS, SH, R, PY, NW, S, RHS>;
+  if ((a.rhs != nullptr) != RHS)
+    return fail(SSAM_ERR_INVALID, "3D kernel instance does not match the right-hand side");
+  static std::mutex mu;
+  static std::map<int, int> ctas_per_sm;  // per device
+  int dev = 0;
+  SSAM_CUDA_TRY(cudaGetDevice(&dev));
+  int bps, sms;
+  {
+    std::lock_guard<std::mutex> g(mu);
+    auto it = ctas_per_sm.find(dev);
+    if (it == ctas_per_sm.end()) {
+      SSAM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         C::SMEM));
+      int b = 0;
+      SSAM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, C::THREADS,
+                                                                  C::SMEM));
+      if (b < 1) return fail(SSAM_ERR_UNSUPPORTED, "3D kernel does not fit on an SM");
+      it = ctas_per_sm.emplace(dev, b).first;
+    }
+    bps = it->second;
+  }
+  SSAM_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+
+  const size_t es = sizeof(TS);
+  Work3D w;
+  w.nx = a.nx;
+  w.ny = a.ny;
+  w.nz = a.nz;
+  w.nb = a.nb;
+  w.rhs = a.rhs;
+  w.rhs_scale = a.rhs_scale;
+  w.ntx = (int)((a.nx + C::TX - 1) / C::TX);
+  w.nty = (int)((a.ny + C::TY - 1) / C::TY);
+  // z chunk: minimise (rounds of items) x (chunk + 2R prologue planes)
+  const int64_t grid_max = (int64_t)sms * bps;
+  const int64_t ntiles = (int64_t)w.ntx * w.nty;
+  int64_t best = -1;
+  for (int zc : {8, 12, 16, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512}) {
+    if (zc > 2 * a.nz && zc > 8) break;
+    const int64_t items = ntiles * ((a.nz + zc - 1) / zc) * a.nb;
+    const int64_t rounds = (items + grid_max - 1) / grid_max;
+    const int64_t cost = rounds * (std::min<int64_t>(zc, a.nz) + 2 * R);
+    if (best < 0 || cost < best) {
+      best = cost;
+      w.zc = zc;
+      w.items = items;
+    }
+  }
+  const int64_t grid = std::min(w.items, grid_max);
+  w.boundary = a.boundary;
+  w.wait_ns = 1000ull * 1000ull * 1000ull;  // 1 s per wait; healthy waits take microseconds
+  int st = device_error_word(&w.err);
+  if (st != SSAM_OK) return st;
+  if (a.prepare_only) return SSAM_OK;
+
+  CUtensorMap map;
+  memset(&map, 0, sizeof(map));
+  w.use_tma = ((uintptr_t)a.src % 16 == 0) && ((a.nx * (int64_t)es) % 16 == 0) &&
+              a.nx <= (int64_t(1) << 32) && tensor_map_encoder() != nullptr;
+  if (w.use_tma) {
+    cuuint64_t dims[4] = {(cuuint64_t)a.nx, (cuuint64_t)a.ny, (cuuint64_t)a.nz,
+                          (cuuint64_t)a.nb};
+    cuuint64_t strides[3] = {(cuuint64_t)(a.nx * es), (cuuint64_t)(a.nx * a.ny * es),
+                             (cuuint64_t)(a.nx * a.ny * a.nz * es)};
+    cuuint32_t box[4] = {(cuuint32_t)C::XW, (cuuint32_t)C::YW, 1, 1};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = tensor_map_encoder()(&map, tma_dtype<TS>(), 4, const_cast<void*>(a.src), dims,
+                             strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) w.use_tma = 0;  // fall back to plain loads
+  }
+  CoefBlock<TA, C::NC> cf;
+  for (int k = 0; k < C::NC; ++k) cf.c[k] = (TA)a.coef[k];
+  kern<<<(unsigned)grid, C::THREADS, C::SMEM, a.stream>>>(map, (const TS*)a.src, (TS*)a.dst,
+                                                          w, cf);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(a.stream, &cap);
+  if (cap == cudaStreamCaptureStatusNone) count_launch();  // graphs count at replay
+  SSAM_CUDA_TRY(cudaGetLastError());
+  return SSAM_OK;
+}
+
+using LaunchFn3D = int (*)(const Launch3D&);
+
+// One compiled configuration of a 3D stencil: rows per consumer warp (PY),
+// consumer warps per CTA (NW; the column tile is 128 x NW*PY) and ring slots
+// (S planes of the tile in shared memory).  `dflt` marks the configuration
+// used when nothing was measured for the grid's size class.
+struct Cand3D {
+  LaunchFn3D fn;
+  int py, nw, s;
+  bool dflt;
+};
+
+// Adds a configuration to the table of (dtype, shape, radius, rhs term).
+void register_3d(int dtype, int shape, int r, bool rhs, const Cand3D& c);
+
+template <typename TS, int SH, int R, int PY, int NW, int S, bool RHS, bool DEFAULT>
+struct Register3D {
+  Register3D() {
+    register_3d(Traits<TS>::DT, SH, R, RHS,
+                Cand3D{&launch_3d<TS, SH, R, PY, NW, S, RHS>, PY, NW, S, DEFAULT});
+  }
+};
+
+}  // namespace ssam
