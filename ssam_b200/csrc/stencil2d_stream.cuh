@@ -41,6 +41,9 @@ struct Stream2DCfg {
   // in local memory
   static constexpr int D = FH >= 13 ? 1 : 4;
   static constexpr int L = FH + D;  // ring length = unroll factor
+  // rows beyond the ones in flight that are prefetched into L2 (no registers
+  // held), so that the loads D rows ahead find their lines on chip
+  static constexpr int PF = 8;
   // rows a warp walks: SEG rounded up to whole ring lengths
   static constexpr int SEGL = (SEG + L - 1) / L * L;
   static_assert(OUT_LANES >= 2, "radius too large for one warp strip");
@@ -63,22 +66,15 @@ __device__ __forceinline__ void stream_unpack(TA (&d)[V], const uint4 (&w)[CH]) 
   }
 }
 
-// Row y of the lane's (clamped) chunk as raw 16-byte words; rows outside the
-// grid are zero (ZERO) or the clamped edge row (CLAMP, COPY).
-template <typename TS, int CH>
-__device__ __forceinline__ void stream_load_row(uint4 (&w)[CH], const TS* __restrict__ src,
-                                                int64_t y, int64_t xc, int64_t H,
-                                                int64_t pitch, int bnd) {
-  const bool y_out = y < 0 || y >= H;
-  const uint4* row =
-      reinterpret_cast<const uint4*>(src + (y < 0 ? 0 : (y >= H ? H - 1 : y)) * pitch + xc);
-  if (y_out && bnd == SSAM_BOUNDARY_ZERO) {
+// 16 zero bytes per 16-byte word of a row chunk (up to 32-byte chunks): rows
+// outside the grid under the ZERO rule are loaded from here, so that every
+// row of the ring is one plain load from a selected pointer.
+__device__ __align__(16) const uint4 g_stream_zero[2] = {};
+
+template <int CH>
+__device__ __forceinline__ void stream_load(uint4 (&w)[CH], const void* p) {
 #pragma unroll
-    for (int c = 0; c < CH; ++c) w[c] = make_uint4(0u, 0u, 0u, 0u);
-  } else {
-#pragma unroll
-    for (int c = 0; c < CH; ++c) w[c] = __ldg(row + c);
-  }
+  for (int c = 0; c < CH; ++c) w[c] = __ldg(reinterpret_cast<const uint4*>(p) + c);
 }
 
 // Values of an outside lane's columns after unpacking the (clamped) edge
@@ -108,7 +104,8 @@ stencil2d_stream_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int64_
                                   Stream2DCfg<TS, RL, RR, RT, RB, STAR, SEG, V_>::NC> cf) {
   using C = Stream2DCfg<TS, RL, RR, RT, RB, STAR, SEG, V_>;
   using TA = typename C::TA;
-  constexpr int V = C::V, FW = C::FW, FH = C::FH, CH = C::CH, D = C::D, L = C::L;
+  constexpr int V = C::V, FW = C::FW, FH = C::FH, CH = C::CH, D = C::D, L = C::L,
+                PF = C::PF;
   constexpr int SEGL = C::SEGL;
   constexpr unsigned FULL = 0xffffffffu;
   const int64_t warp_x = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -124,36 +121,63 @@ stencil2d_stream_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int64_
   const bool edge_warp = x_out0 - (int64_t)C::HL * V < 0 || x_out0 + (32 - C::HL) * V > W;
   // columns of this lane that the COPY rule keeps at their input value
   const bool x_copy = bnd == SSAM_BOUNDARY_COPY && (x0 < RL || x0 + V > W - RR);
-  const int64_t nseg = (y_end - y_begin + SEGL - 1) / SEGL;
+  const int nseg = (int)((y_end - y_begin + SEGL - 1) / SEGL);
+  // rows outside the grid: the clamped edge row of this lane's chunk (CLAMP,
+  // COPY) or zeros (ZERO)
+  const TS* const row_top =
+      bnd == SSAM_BOUNDARY_ZERO ? reinterpret_cast<const TS*>(g_stream_zero) : src + xc;
+  const TS* const row_bot = bnd == SSAM_BOUNDARY_ZERO
+                                ? reinterpret_cast<const TS*>(g_stream_zero)
+                                : src + (H - 1) * pitch + xc;
+  const int h = (int)H;  // H, W < 2^31 (checked by the entry points)
+  const bool fix_lane = edge_warp && where != kLaneIn;
+  const bool copy = bnd == SSAM_BOUNDARY_COPY;
 
-  for (int64_t sg = blockIdx.y; sg < nseg; sg += gridDim.y) {
-    const int64_t ya = y_begin + sg * SEGL;  // first output row of the segment
+  for (int sg = blockIdx.y; sg < nseg; sg += gridDim.y) {
+    const int ya = (int)y_begin + sg * SEGL;  // first output row of the segment
     // ring slot of grid row ya + k (k >= -RT) is (k + RT) % L
     uint4 raw[L][CH];
     TA val[L][V];
     // prologue: rows ya-RT .. ya+RB+D-1 in flight, ya-RT .. ya+RB-1 converted
 #pragma unroll
-    for (int k = 0; k < FH - 1 + D; ++k) stream_load_row<TS, CH>(raw[k], src, ya - RT + k, xc, H, pitch, bnd);
+    for (int k = 0; k < FH - 1 + D; ++k) {
+      const int y = ya - RT + k;
+      stream_load<CH>(raw[k], (unsigned)y < (unsigned)h ? src + (int64_t)y * pitch + xc
+                                                        : (y < 0 ? row_top : row_bot));
+    }
 #pragma unroll
     for (int k = 0; k < FH - 1; ++k) {
       stream_unpack<TS, V, CH>(val[k], raw[k]);
-      if (edge_warp && where != kLaneIn) stream_fix_lane<V>(val[k], where, bnd);
+      if (fix_lane) stream_fix_lane<V>(val[k], where, bnd);
     }
 
     // whole groups of L rows (rows past y_end are computed, not stored)
-    const int64_t left = y_end - ya;
-    const int nrows = left < SEGL ? (int)left : SEGL;
+    const int left = (int)y_end - ya;
+    const int nrows = left < SEGL ? left : SEGL;
+    // rows ya + k, k < pf_rows, are read by this segment and inside the grid
+    const int pf_rows = (h - ya) < nrows + RB ? (h - ya) : nrows + RB;
+    const TS* ldp = src + (int64_t)(ya + RB + D) * pitch + xc;  // next ring load
+    const TS* pfp = ldp + (int64_t)PF * pitch;                   // next L2 prefetch
+    TS* stp = dst + (int64_t)ya * pitch + x0;                    // next store
     for (int base = 0; base < nrows; base += L) {
 #pragma unroll
       for (int u = 0; u < L; ++u) {
         const int i = base + u;  // output row ya + i
         // the row D ahead of the reach; its slot held row ya+i-RT-1, now done
-        stream_load_row<TS, CH>(raw[(u + FH - 1 + D) % L], src, ya + i + RB + D, xc, H,
-                                pitch, bnd);
+        {
+          const int y = ya + i + RB + D;
+          stream_load<CH>(raw[(u + FH - 1 + D) % L],
+                          (unsigned)y < (unsigned)h ? ldp : (y < 0 ? row_top : row_bot));
+          ldp += pitch;
+        }
+        // L2 prefetch PF rows further on, within the rows this segment reads
+        asm volatile(
+            "{ .reg .pred q; setp.lt.s32 q, %1, %2; @q prefetch.global.L2 [%0]; }" ::"l"(pfp),
+            "r"(i + RB + D + PF), "r"(pf_rows));
+        pfp += pitch;
         // the row entering the reach
         stream_unpack<TS, V, CH>(val[(u + FH - 1) % L], raw[(u + FH - 1) % L]);
-        if (edge_warp && where != kLaneIn)
-          stream_fix_lane<V>(val[(u + FH - 1) % L], where, bnd);
+        if (fix_lane) stream_fix_lane<V>(val[(u + FH - 1) % L], where, bnd);
 
         TA acc[V];
 #pragma unroll
@@ -230,16 +254,17 @@ stencil2d_stream_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int64_
             }
           }
         }
-        const int64_t y = ya + i;
-        if (bnd == SSAM_BOUNDARY_COPY && (x_copy || y < RT || y >= H - RB)) {
+        const int y = ya + i;
+        if (copy && (x_copy || (unsigned)(y - RT) >= (unsigned)(h - RT - RB))) {
+          const bool y_ring = (unsigned)(y - RT) >= (unsigned)(h - RT - RB);
 #pragma unroll
           for (int j = 0; j < V; ++j) {
             const int64_t x = x0 + j;
-            if ((x < RL) | (x >= W - RR) | (y < RT) | (y >= H - RB))
-              acc[j] = val[(u + RT) % L][j];
+            if (y_ring | (x < RL) | (x >= W - RR)) acc[j] = val[(u + RT) % L][j];
           }
         }
-        if (lane_stores && y < y_end) store_vec<TS, V>(dst + y * pitch + x0, acc);
+        if (lane_stores && y < (int)y_end) store_vec<TS, V>(stp, acc);
+        stp += pitch;
       }
     }
   }
