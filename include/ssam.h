@@ -265,6 +265,8 @@ typedef struct ssam_tune3d_report {
   int rows_per_warp;  /* PY: rows of the column tile each consumer warp computes */
   int consumer_warps; /* NW: consumer warps per CTA; the tile is 128 x NW*PY cells */
   int ring_slots;     /* S: z-planes of the tile staged in shared memory */
+  int registers_z;    /* 1: each thread keeps its own cells of the 2R+1 planes in
+                         registers (shared memory carries the halos only) */
   int candidates;     /* configurations timed */
   double ms_per_step; /* best measured time of one launch (ms) */
 } ssam_tune3d_report;

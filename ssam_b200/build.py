@@ -74,32 +74,37 @@ def instances():
 
 
 def instances_3d():
-    """(dtype, shape, r, PY, NW, S, rhs, default) of every compiled 3D
+    """(dtype, shape, r, PY, NW, S, rhs, default, zreg) of every compiled 3D
     configuration: shape 0 = star (r = 1: 7-pt, r = 2: 13-pt), 1 = the
     19-point Poisson operator; rhs = the Jacobi-sweep form with a
-    right-hand-side term.  The first of each group is the default; the 3D
-    autotuner times them all."""
+    right-hand-side term; zreg = the kernel that keeps each thread's own
+    cells in a register ring along z (stencil3d_zreg.cuh; "z" below).  The
+    first of each group is the default; the 3D autotuner times them all."""
     cfg = {
-        "f32": {(0, 1): [(4, 8, 6), (4, 4, 8), (2, 16, 6), (4, 16, 5), (8, 8, 5)],
-                (0, 2): [(4, 4, 8), (4, 8, 6), (2, 8, 6), (2, 16, 6), (4, 12, 6)],
-                (1, 1): [(4, 8, 6), (4, 4, 8), (2, 16, 6), (4, 16, 5)],
-                "rhs": [(4, 8, 6), (4, 4, 8), (2, 16, 6), (4, 16, 5)]},
-        "bf16": {(0, 1): [(4, 8, 6), (2, 16, 6), (4, 16, 6), (8, 8, 6)],
-                 (0, 2): [(4, 4, 8), (4, 8, 6), (2, 16, 6)],
-                 (1, 1): [(4, 8, 6), (2, 16, 6), (4, 16, 6)],
-                 "rhs": [(4, 8, 6), (2, 16, 6), (4, 16, 6)]},
-        "f64": {(0, 1): [(4, 4, 5), (4, 8, 5), (2, 8, 5)],
-                (0, 2): [(4, 4, 6), (2, 8, 6)],
-                (1, 1): [(4, 4, 5), (2, 8, 5)],
-                "rhs": [(4, 4, 5), (2, 8, 5)]},
+        "f32": {(0, 1): [(4, 8, 6), (4, 4, 8), (2, 16, 6), (4, 16, 5), (8, 8, 5),
+                         (2, 16, 4, "z"), (2, 8, 4, "z")],
+                (0, 2): [(4, 4, 8), (4, 8, 6), (2, 8, 6), (2, 16, 6), (4, 12, 6),
+                         (2, 12, 4, "z"), (2, 16, 4, "z")],
+                (1, 1): [(4, 8, 6), (4, 4, 8), (2, 16, 6), (4, 16, 5),
+                         (2, 16, 4, "z"), (2, 8, 4, "z")],
+                "rhs": [(4, 8, 6), (4, 4, 8), (2, 16, 6), (4, 16, 5),
+                        (2, 16, 4, "z"), (2, 8, 4, "z")]},
+        "bf16": {(0, 1): [(4, 8, 6), (2, 16, 6), (4, 16, 6), (8, 8, 6), (2, 16, 4, "z")],
+                 (0, 2): [(4, 4, 8), (4, 8, 6), (2, 16, 6), (2, 12, 4, "z")],
+                 (1, 1): [(4, 8, 6), (2, 16, 6), (4, 16, 6), (2, 16, 4, "z")],
+                 "rhs": [(4, 8, 6), (2, 16, 6), (4, 16, 6), (2, 16, 4, "z"), (2, 8, 4, "z")]},
+        "f64": {(0, 1): [(4, 4, 5), (4, 8, 5), (2, 8, 5), (2, 4, 4, "z")],
+                (0, 2): [(4, 4, 6), (2, 8, 6), (2, 4, 4, "z")],
+                (1, 1): [(4, 4, 5), (2, 8, 5), (2, 4, 4, "z")],
+                "rhs": [(4, 4, 5), (2, 8, 5), (2, 4, 4, "z")]},
         "f16": {(0, 1): [(4, 8, 6)], (0, 2): [(4, 4, 8)], (1, 1): [(4, 8, 6)]},
     }
     out = []
     for dt, groups in cfg.items():
         for key, lst in groups.items():
             shape, r, rhs = (0, 1, True) if key == "rhs" else (key[0], key[1], False)
-            for i, (py, nw, s) in enumerate(lst):
-                out.append((dt, shape, r, py, nw, s, rhs, i == 0))
+            for i, c in enumerate(lst):
+                out.append((dt, shape, r, c[0], c[1], c[2], rhs, i == 0, len(c) > 3))
     return out
 
 
@@ -153,12 +158,13 @@ def _gen_units(chunk: int = 6):
             name = f"inst3d_{dt}_{c // 3:02d}.cu"
             lines = ["// generated by ssam_b200/build.py -- do not edit",
                      '#include "../../csrc/stencil3d_launch.cuh"', "namespace ssam {"]
-            for (_, shape, r, py, nw, s, rhs, dflt) in part:
+            for (_, shape, r, py, nw, s, rhs, dflt, zreg) in part:
                 sh = "SH3_POISSON19" if shape else "SH3_STAR"
-                tag = f"{shape}_{r}_{py}_{nw}_{s}_{int(rhs)}"
+                tag = f"{shape}_{r}_{py}_{nw}_{s}_{int(rhs)}_{int(zreg)}"
                 lines.append(
                     f"static Register3D<{DTYPES[dt]}, {sh}, {r}, {py}, {nw}, {s}, "
-                    f"{'true' if rhs else 'false'}, {'true' if dflt else 'false'}> reg3_{tag};")
+                    f"{'true' if rhs else 'false'}, {'true' if dflt else 'false'}, "
+                    f"{'true' if zreg else 'false'}> reg3_{tag};")
             lines.append("}  // namespace ssam")
             text = "\n".join(lines) + "\n"
             path = os.path.join(BUILD, "gen", name)

@@ -83,7 +83,6 @@ struct Stencil3DCfg {
   // shared memory and the CTA is at most 9 warps, else one
   static constexpr int MINB = (NW < 12 && 2 * (SMEM + 1024) <= 233472) ? 2 : 1;
   static_assert(R <= HX && R <= V, "x reach must fit in the halo and one lane hop");
-  static_assert(S >= 2 * R + 2, "ring must hold the stencil window plus one plane");
 };
 
 struct Work3D {
@@ -217,6 +216,63 @@ __device__ __forceinline__ Seg3D item_seg(int64_t it, const Work3D& w) {
   return s;
 }
 
+// The producer warp of a 3D CTA: stages every plane of every work item of
+// this CTA -- planes za-R .. zb+R-1 of the item's column tile, halos included
+// -- into the ring of S slots, in order.  A slot is reused once the consumer
+// warps have released its previous plane (empty barrier); a TMA copy signals
+// `full` by bytes, the plain-load path by 32 arrivals.  Every wait is
+// bounded: on expiry the error word is set and staging stops.  Before
+// returning, the last use of every slot must have landed.
+template <typename TS, int R, int S, typename C>
+__device__ __forceinline__ void produce_planes(const CUtensorMap& map, const TS* __restrict__ src,
+                                               const Work3D& w, TS* slots, uint64_t* full,
+                                               uint64_t* empty, int lane) {
+  using TA = typename C::TA;
+  constexpr int XW = C::XW, HX = C::HX, RYM = C::RYM, TY = C::TY;
+  const int64_t nx = w.nx, ny = w.ny, nz = w.nz, nxy = nx * ny;
+  uint32_t n = 0;  // planes issued so far (ring position)
+  bool ok = true;
+  for (int64_t it = blockIdx.x; ok && it < w.items; it += gridDim.x) {
+    const Seg3D sg = item_seg(it, w);
+    const int tx = (int)(sg.tile % w.ntx), ty = (int)(sg.tile / w.ntx);
+    const int gx = tx * C::TX - HX, gy = ty * TY - RYM;
+    for (int64_t p = sg.za - R; p < sg.zb + R; ++p, ++n) {
+      const int s = n % S;
+      const unsigned use = n / S;
+      if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1, w.wait_ns)) {
+        if (lane == 0) atomicCAS(w.err, 0, 1);
+        ok = false;
+        break;
+      }
+      TS* slot = slots + (size_t)s * (C::SLOT_BYTES / sizeof(TS));
+      if (w.use_tma) {
+        if (lane == 0) {
+          mbar_expect_tx(&full[s], (unsigned)(XW * C::YW * sizeof(TS)));
+          tma_load_plane(slot, &map, gx, gy, (int)p, (int)sg.b, &full[s]);
+        }
+      } else {
+        // plain loads for grids whose rows are not 16-byte multiples
+        for (int i = lane; i < XW * C::YW; i += 32) {
+          const int r = i / XW, c = i % XW;
+          const int64_t x = gx + c, y = gy + r;
+          TS v = from_acc<TS>(TA(0));
+          if (x >= 0 && x < nx && y >= 0 && y < ny && p >= 0 && p < nz)
+            v = src[(sg.b * nz + p) * nxy + y * nx + x];
+          slot[r * XW + c] = v;
+        }
+        mbar_arrive(&full[s]);
+      }
+      __syncwarp();
+    }
+  }
+  // drain: the last use of every slot must have landed before exit
+  if (w.use_tma && lane == 0) {
+    const uint32_t first = n > (uint32_t)S ? n - S : 0;
+    for (uint32_t k = first; k < n; ++k)
+      if (!mbar_wait(&full[k % S], (k / S) & 1, w.wait_ns)) atomicCAS(w.err, 0, 2);
+  }
+}
+
 // RHS: the Jacobi form out = stencil(in) + rhs_scale * rhs.  Its rows are
 // loaded at the top of every plane, so their latency overlaps the plane's
 // barrier waits and arithmetic (instances without it carry no rhs code).
@@ -231,6 +287,7 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
   constexpr int V = C::V, XW = C::XW, HX = C::HX, RYM = C::RYM, TY = C::TY;
   constexpr int F = 2 * R + 1;
   constexpr unsigned FULL = 0xffffffffu;
+  static_assert(S >= 2 * R + 2, "ring must hold the stencil window plus one plane");
 
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char* base =
@@ -252,48 +309,7 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
   const int64_t nx = w.nx, ny = w.ny, nz = w.nz, nxy = nx * ny;
 
   if (warp == NW) {
-    // ------------------------------------------------------ producer warp
-    uint32_t n = 0;  // planes issued so far (ring position)
-    bool ok = true;
-    for (int64_t it = blockIdx.x; ok && it < w.items; it += gridDim.x) {
-      const Seg3D sg = item_seg(it, w);
-      const int tx = (int)(sg.tile % w.ntx), ty = (int)(sg.tile / w.ntx);
-      const int gx = tx * C::TX - HX, gy = ty * TY - RYM;
-      for (int64_t p = sg.za - R; p < sg.zb + R; ++p, ++n) {
-        const int s = n % S;
-        const unsigned use = n / S;
-        if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1, w.wait_ns)) {
-          if (lane == 0) atomicCAS(w.err, 0, 1);
-          ok = false;
-          break;
-        }
-        TS* slot = slots + (size_t)s * (C::SLOT_BYTES / sizeof(TS));
-        if (w.use_tma) {
-          if (lane == 0) {
-            mbar_expect_tx(&full[s], (unsigned)(XW * C::YW * sizeof(TS)));
-            tma_load_plane(slot, &map, gx, gy, (int)p, (int)sg.b, &full[s]);
-          }
-        } else {
-          // plain loads for grids whose rows are not 16-byte multiples
-          for (int i = lane; i < XW * C::YW; i += 32) {
-            const int r = i / XW, c = i % XW;
-            const int64_t x = gx + c, y = gy + r;
-            TS v = from_acc<TS>(TA(0));
-            if (x >= 0 && x < nx && y >= 0 && y < ny && p >= 0 && p < nz)
-              v = src[(sg.b * nz + p) * nxy + y * nx + x];
-            slot[r * XW + c] = v;
-          }
-          mbar_arrive(&full[s]);
-        }
-        __syncwarp();
-      }
-    }
-    // drain: the last use of every slot must have landed before exit
-    if (w.use_tma && lane == 0) {
-      const uint32_t first = n > (uint32_t)S ? n - S : 0;
-      for (uint32_t k = first; k < n; ++k)
-        if (!mbar_wait(&full[k % S], (k / S) & 1, w.wait_ns)) atomicCAS(w.err, 0, 2);
-    }
+    produce_planes<TS, R, S, C>(map, src, w, slots, full, empty, lane);
     return;
   }
 

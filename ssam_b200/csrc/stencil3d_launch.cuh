@@ -10,7 +10,7 @@
 #include <map>
 #include <mutex>
 
-#include "stencil3d.cuh"
+#include "stencil3d_zreg.cuh"
 
 namespace ssam {
 
@@ -44,11 +44,17 @@ struct Launch3D {
   bool prepare_only;  // resolve attributes/occupancy/symbols, launch nothing
 };
 
-template <typename TS, int SH, int R, int PY, int NW, int S, bool RHS = false>
+// ZREG: the kernel of stencil3d_zreg.cuh (own cells in a register ring
+// along z) instead of stencil3d_kernel.
+template <typename TS, int SH, int R, int PY, int NW, int S, bool RHS = false,
+          bool ZREG = false>
 int launch_3d(const Launch3D& a) {
   using C = Stencil3DCfg<TS, SH, R, PY, NW, S>;
   using TA = typename C::TA;
-  auto kern = stencil3d_kernel<TS, SH, R, PY, NW, S, RHS>;
+  auto kern = [] {
+    if constexpr (ZREG) return &stencil3d_zreg_kernel<TS, SH, R, PY, NW, S, RHS>;
+    else return &stencil3d_kernel<TS, SH, R, PY, NW, S, RHS>;
+  }();
   if ((a.rhs != nullptr) != RHS)
     return fail(SSAM_ERR_INVALID, "3D kernel instance does not match the right-hand side");
   static std::mutex mu;
@@ -135,23 +141,26 @@ int launch_3d(const Launch3D& a) {
 using LaunchFn3D = int (*)(const Launch3D&);
 
 // One compiled configuration of a 3D stencil: rows per consumer warp (PY),
-// consumer warps per CTA (NW; the column tile is 128 x NW*PY) and ring slots
-// (S planes of the tile in shared memory).  `dflt` marks the configuration
+// consumer warps per CTA (NW; the column tile is 128 x NW*PY), ring slots
+// (S planes of the tile in shared memory) and the kernel variant.  `dflt` marks the configuration
 // used when nothing was measured for the grid's size class.
 struct Cand3D {
   LaunchFn3D fn;
   int py, nw, s;
+  int zreg;  // 1: own cells in a register ring along z (stencil3d_zreg.cuh)
   bool dflt;
 };
 
 // Adds a configuration to the table of (dtype, shape, radius, rhs term).
 void register_3d(int dtype, int shape, int r, bool rhs, const Cand3D& c);
 
-template <typename TS, int SH, int R, int PY, int NW, int S, bool RHS, bool DEFAULT>
+template <typename TS, int SH, int R, int PY, int NW, int S, bool RHS, bool DEFAULT,
+          bool ZREG = false>
 struct Register3D {
   Register3D() {
     register_3d(Traits<TS>::DT, SH, R, RHS,
-                Cand3D{&launch_3d<TS, SH, R, PY, NW, S, RHS>, PY, NW, S, DEFAULT});
+                Cand3D{&launch_3d<TS, SH, R, PY, NW, S, RHS, ZREG>, PY, NW, S, ZREG ? 1 : 0,
+                       DEFAULT});
   }
 };
 

@@ -1,5 +1,6 @@
 """Every compiled 3D configuration (rows per warp PY, consumer warps NW,
-ring slots S) against the oracle, and the 3D autotuners.
+ring slots S, and the variant with each thread's own cells in a register
+ring along z) against the oracle, and the 3D autotuners.
 
 A configuration is pinned for the grid's size class through a tune-cache
 file (``choice3d`` lines, read by ssam_autotune_load), the public way to fix
@@ -30,20 +31,20 @@ def log2(v):
 
 
 def pin(tmp_path, dt, shape, r, rhs, nx, ny, nzb, cfg):
-    py, nw, s = cfg
+    py, nw, s, zreg = cfg
     p = tmp_path / "pin3d.txt"
     p.write_text("# ssam_b200 autotune cache v1\n"
                  f"choice3d {DTC[dt]} {shape} {r} {int(rhs)} {log2(nx)} {log2(ny)} {log2(nzb)} "
-                 f"{py} {nw} {s}\n")
+                 f"{py} {nw} {s} {int(zreg)}\n")
     S.autotune_clear()
     S.autotune_load(str(p))
 
 
 def stencil_cases():
     out = []
-    for (dt, shape, r, py, nw, s, rhs, _) in instances_3d():
+    for (dt, shape, r, py, nw, s, rhs, _, zreg) in instances_3d():
         if not rhs and dt in ("f32", "f64", "bf16"):
-            out.append((dt, shape, r, (py, nw, s)))
+            out.append((dt, shape, r, (py, nw, s, zreg)))
     return out
 
 
@@ -81,7 +82,8 @@ def test_every_3d_configuration_vs_oracle(cuda, tmp_path, dt, shape, r, cfg, dim
 
 
 def sweep_cases():
-    return [(dt, (py, nw, s)) for (dt, shape, r, py, nw, s, rhs, _) in instances_3d() if rhs]
+    return [(dt, (py, nw, s, zreg)) for (dt, shape, r, py, nw, s, rhs, _, zreg) in instances_3d()
+            if rhs]
 
 
 @pytest.mark.parametrize("dt,cfg", sweep_cases())
