@@ -82,21 +82,23 @@ def instances_3d():
     first of each group is the default; the 3D autotuner times them all."""
     cfg = {
         "f32": {(0, 1): [(4, 8, 6), (4, 4, 8), (2, 16, 6), (4, 16, 5), (8, 8, 5),
-                         (2, 16, 4, "z"), (2, 8, 4, "z")],
-                (0, 2): [(4, 4, 8), (4, 8, 6), (2, 8, 6), (2, 16, 6), (4, 12, 6),
-                         (2, 12, 4, "z"), (2, 16, 4, "z")],
-                (1, 1): [(4, 8, 6), (4, 4, 8), (2, 16, 6), (4, 16, 5),
-                         (2, 16, 4, "z"), (2, 8, 4, "z")],
+                         (2, 16, 4, "z"), (2, 8, 4, "z"), (2, 16, 8, "z"), (2, 8, 8, "z")],
+                (0, 2): [(4, 4, 8), (4, 8, 6), (2, 8, 6), (2, 16, 6), (4, 12, 6), (4, 12, 8),
+                         (2, 12, 4, "z"), (2, 16, 4, "z"), (2, 16, 8, "z"), (2, 12, 8, "z")],
+                (1, 1): [(4, 8, 6), (4, 4, 8), (2, 16, 6), (4, 16, 5), (4, 8, 8),
+                         (2, 16, 4, "z"), (2, 8, 4, "z"), (2, 16, 8, "z")],
                 "rhs": [(4, 8, 6), (4, 4, 8), (2, 16, 6), (4, 16, 5),
-                        (2, 16, 4, "z"), (2, 8, 4, "z")]},
-        "bf16": {(0, 1): [(4, 8, 6), (2, 16, 6), (4, 16, 6), (8, 8, 6), (2, 16, 4, "z")],
-                 (0, 2): [(4, 4, 8), (4, 8, 6), (2, 16, 6), (2, 12, 4, "z")],
-                 (1, 1): [(4, 8, 6), (2, 16, 6), (4, 16, 6), (2, 16, 4, "z")],
-                 "rhs": [(4, 8, 6), (2, 16, 6), (4, 16, 6), (2, 16, 4, "z"), (2, 8, 4, "z")]},
-        "f64": {(0, 1): [(4, 4, 5), (4, 8, 5), (2, 8, 5), (2, 4, 4, "z")],
-                (0, 2): [(4, 4, 6), (2, 8, 6), (2, 4, 4, "z")],
-                (1, 1): [(4, 4, 5), (2, 8, 5), (2, 4, 4, "z")],
-                "rhs": [(4, 4, 5), (2, 8, 5), (2, 4, 4, "z")]},
+                        (2, 16, 4, "z"), (2, 8, 4, "z"), (2, 16, 8, "z"), (2, 8, 8, "z")]},
+        "bf16": {(0, 1): [(4, 8, 6), (2, 16, 6), (4, 16, 6), (8, 8, 6), (2, 16, 4, "z"),
+                          (2, 16, 8, "z")],
+                 (0, 2): [(4, 4, 8), (4, 8, 6), (2, 16, 6), (2, 12, 4, "z"), (2, 16, 8, "z")],
+                 (1, 1): [(4, 8, 6), (2, 16, 6), (4, 16, 6), (2, 16, 4, "z"), (2, 16, 8, "z")],
+                 "rhs": [(4, 8, 6), (2, 16, 6), (4, 16, 6), (2, 16, 4, "z"), (2, 8, 4, "z"),
+                         (2, 16, 8, "z")]},
+        "f64": {(0, 1): [(4, 4, 5), (4, 8, 5), (2, 8, 5), (2, 4, 4, "z"), (2, 8, 8, "z")],
+                (0, 2): [(4, 4, 6), (2, 8, 6), (2, 4, 4, "z"), (2, 8, 8, "z")],
+                (1, 1): [(4, 4, 5), (2, 8, 5), (2, 4, 4, "z"), (2, 8, 8, "z")],
+                "rhs": [(4, 4, 5), (2, 8, 5), (2, 4, 4, "z"), (2, 8, 8, "z")]},
         "f16": {(0, 1): [(4, 8, 6)], (0, 2): [(4, 4, 8)], (1, 1): [(4, 8, 6)]},
     }
     out = []
