@@ -1105,9 +1105,18 @@ def main(argv=None):
     ap.add_argument("--impl", default="ssam", choices=["ssam", "reference"])
     ap.add_argument("--workload", default=DEFAULT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tuned", default=None, metavar="FILE",
+                    help="load launch choices from a tune-cache file (ssam_autotune_save "
+                         "format) instead of measuring them")
+    ap.add_argument("--save-tuned", default=None, metavar="FILE",
+                    help="save the launch choices this run made (to replay them with --tuned)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="use the built-in launch defaults instead of measuring")
     args = ap.parse_args(argv)
+    if args.tuned:
+        import ssam_b200 as S
+        S.autotune_load(args.tuned)
+        args.no_autotune = True  # replay the loaded choices, measure nothing
     wl = workloads()
     if args.workload not in wl:
         raise SystemExit(f"unknown workload {args.workload}; known: {sorted(wl)}")
@@ -1124,6 +1133,9 @@ def main(argv=None):
         run_jacobi(args, spec, args.workload)
     else:
         run_ssam(args, spec, args.workload)
+    if args.save_tuned and args.impl != "reference":
+        import ssam_b200 as S
+        S.autotune_save(args.save_tuned)
 
 
 if __name__ == "__main__":

@@ -22,7 +22,7 @@
 #include <vector>
 
 #include "autotune.h"
-#include "stencil2d.cuh"
+#include "stencil2d_stream.cuh"
 
 namespace ssam {
 
@@ -122,6 +122,36 @@ batched_kernel(BatchWork w, CoefBlock<typename Traits<TS>::TA, (2 * R + 1) * (2 
   }
 }
 
+// The same with row-streaming warp tiles (stencil2d_stream.cuh): a work item
+// is one SEG-row segment of one warp strip of one grid; single steps only.
+// Every grid must have 16-byte aligned buffers and a pitch that is a multiple
+// of V (checked by the entry point).
+template <typename TS, int R, bool STAR, int SEG, int V>
+__global__ void __launch_bounds__(128)
+batched_stream_kernel(BatchWork w,
+                      CoefBlock<typename Traits<TS>::TA, (2 * R + 1) * (2 * R + 1)> cf) {
+  using C = Stream2DCfg<TS, R, R, R, R, STAR, SEG, V>;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  for (int ph = 0; ph < w.nphases; ++ph) {
+    const bool out_dst = ((w.nphases - 1 - ph + w.phases_after) % 2) == 0;
+    int g = 0;
+    for (int64_t it = gw; it < w.items; it += nwarps) {
+      while (g + 1 < w.ngrids && w.grids[g + 1].item0 <= it) ++g;
+      const BatchGrid& bg = w.grids[g];
+      const int64_t local = it - bg.item0;
+      const int64_t wx = local % bg.nwx, sgi = local / bg.nwx;
+      const TS* in = ph == 0 ? (const TS*)bg.first_in
+                             : (const TS*)(out_dst ? bg.scratch : bg.dst);
+      TS* out = out_dst ? (TS*)bg.dst : (TS*)bg.scratch;
+      stream2d_warp_segments<TS, R, R, R, R, STAR, SEG, V, true>(
+          in, out, bg.w, bg.h, bg.pitch, wx * C::OUT_COLS, 0, bg.h, (int)sgi, 1 << 30, w.bnd,
+          cf);
+    }
+    if (ph + 1 < w.nphases && !batch_barrier(w, (unsigned)ph)) return;
+  }
+}
+
 struct BatchLaunch {
   std::vector<BatchGrid>* grids;  // host copy; item0/nwx/first_in set here
   int nphases;                    // phases of this launch (all of depth TT)
@@ -131,17 +161,26 @@ struct BatchLaunch {
   cudaStream_t stream;
 };
 
-template <typename TS, int R, bool STAR, int P, int TT, int V>
+// STREAM: the row-streaming kernel (P = SEG rows per segment, TT = 1).
+template <typename TS, int R, bool STAR, int P, int TT, int V, bool STREAM = false>
 static int launch_batched(BatchLaunch& a) {
   using TA = typename Traits<TS>::TA;
-  using C = Stencil2DCfg<TS, R, R, R, R, STAR, P, TT, V>;
+  using CW = Stencil2DCfg<TS, R, R, R, R, STAR, P, TT, V>;
+  using CS = Stream2DCfg<TS, R, R, R, R, STAR, P, V>;
   constexpr int NC = (2 * R + 1) * (2 * R + 1);
-  auto kern = batched_kernel<TS, R, STAR, P, TT, V>;
+  constexpr int OUT_COLS = STREAM ? CS::OUT_COLS : CW::OUT_COLS;
+  constexpr int ROWS = STREAM ? CS::SEGL : P;  // rows of one work item
+  static_assert(!STREAM || TT == 1, "streaming tiles take single steps");
+  auto kern = [] {
+    if constexpr (STREAM) return &batched_stream_kernel<TS, R, STAR, P, V>;
+    else return &batched_kernel<TS, R, STAR, P, TT, V>;
+  }();
   std::vector<BatchGrid>& grids = *a.grids;
   BatchWork w;
   int64_t acc = 0;
   for (BatchGrid& g : grids) {
-    g.nwx = (int32_t)((g.w + C::OUT_COLS - 1) / C::OUT_COLS);
+    g.nwx = (int32_t)((g.w + OUT_COLS - 1) / OUT_COLS);
+    g.nby = (int32_t)((g.h + ROWS - 1) / ROWS);
     g.item0 = acc;
     acc += (int64_t)g.nwx * g.nby;
   }
@@ -228,6 +267,31 @@ static BatchFn find_batched(int dtype, int star, int r, int t) {
   return nullptr;
 }
 
+// Single-step streaming kernels (SEG = 32) for the same stencils.
+static BatchFn find_batched_stream(int dtype, int star, int r) {
+#define SSAM_BS(TS, R, ST, V) \
+  if (r == R && star == (ST ? 1 : 0)) return &launch_batched<TS, R, ST, 32, 1, V, true>;
+  switch (dtype) {
+    case SSAM_F32:
+      SSAM_BS(float, 1, true, 4) SSAM_BS(float, 1, false, 4)
+      SSAM_BS(float, 2, true, 4) SSAM_BS(float, 2, false, 4)
+      SSAM_BS(float, 3, true, 4) SSAM_BS(float, 3, false, 4)
+      break;
+    case SSAM_F64:
+      SSAM_BS(double, 1, true, 4) SSAM_BS(double, 1, false, 4)
+      SSAM_BS(double, 2, true, 4) SSAM_BS(double, 2, false, 4)
+      break;
+    case SSAM_BF16:
+      SSAM_BS(__nv_bfloat16, 1, true, 8) SSAM_BS(__nv_bfloat16, 1, false, 8)
+      SSAM_BS(__nv_bfloat16, 2, true, 8) SSAM_BS(__nv_bfloat16, 2, false, 8)
+      break;
+  }
+#undef SSAM_BS
+  return nullptr;
+}
+
+static int stream_width(int dtype) { return dtype == SSAM_BF16 || dtype == SSAM_F16 ? 8 : 4; }
+
 }  // namespace ssam
 
 using namespace ssam;
@@ -270,6 +334,19 @@ extern "C" int ssam_stencil2d_batched(const ssam_grid2d* grids, int ngrids, int 
   const int q = steps / deep, rem = steps % deep;
   BatchFn fn_deep = find_batched(dtype, star, radius, deep);
   BatchFn fn_one = find_batched(dtype, star, radius, 1);
+  // single-step phases stream rows when every grid's rows are whole 16-byte
+  // chunks of V columns (aligned buffers, pitch a multiple of V)
+  bool all_aligned = true;
+  for (int i = 0; i < ngrids; ++i)
+    all_aligned = all_aligned && (uintptr_t)grids[i].src % 16 == 0 &&
+                  (uintptr_t)grids[i].dst % 16 == 0 &&
+                  grids[i].pitch % stream_width(dtype) == 0 &&
+                  (boundary != SSAM_BOUNDARY_CLAMP || grids[i].width % stream_width(dtype) == 0);
+  BatchFn fn_stream = all_aligned ? find_batched_stream(dtype, star, radius) : nullptr;
+  if (fn_stream) {
+    fn_one = fn_stream;
+    if (deep == 1) fn_deep = fn_stream;
+  }
   if (!fn_deep || (rem && !fn_one))
     return fail(SSAM_ERR_UNSUPPORTED,
                 "no persistent batched kernel for this dtype/shape/radius (use "
@@ -297,7 +374,6 @@ extern "C" int ssam_stencil2d_batched(const ssam_grid2d* grids, int ngrids, int 
     g.w = grids[i].width;
     g.h = grids[i].height;
     g.pitch = grids[i].pitch;
-    g.nby = (int32_t)((g.h + 7) / 8);  // P = 8 rows per warp tile (find_batched)
     g.vec_ok = ((uintptr_t)g.first_in % 16 == 0) && ((uintptr_t)g.dst % 16 == 0) &&
                (!g.scratch || (uintptr_t)g.scratch % 16 == 0) &&
                ((g.pitch * (int64_t)es) % 16 == 0);

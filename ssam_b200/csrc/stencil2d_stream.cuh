@@ -50,10 +50,10 @@ struct Stream2DCfg {
   static_assert((V * sizeof(TS)) % 16 == 0, "a thread owns whole 16-byte chunks");
 };
 
-// Where a lane's V columns lie: all inside the grid, or (grids whose width is
-// a multiple of V, which the streaming kernel requires) all outside it, left
-// or right.
-enum StreamLane { kLaneIn = 0, kLaneLeft = 1, kLaneRight = 2 };
+// Where a lane's V columns lie: all inside the grid, all outside it (left or
+// right), or -- the last chunk of a row whose width is not a multiple of V --
+// partly inside.
+enum StreamLane { kLaneIn = 0, kLaneLeft = 1, kLaneRight = 2, kLanePartial = 3 };
 
 template <typename TS, int V, int CH, typename TA>
 __device__ __forceinline__ void stream_unpack(TA (&d)[V], const uint4 (&w)[CH]) {
@@ -71,53 +71,79 @@ __device__ __forceinline__ void stream_unpack(TA (&d)[V], const uint4 (&w)[CH]) 
 // row of the ring is one plain load from a selected pointer.
 __device__ __align__(16) const uint4 g_stream_zero[2] = {};
 
+// `chv` = 16-byte words of the chunk that hold a column inside the grid (the
+// others of a row's last, partial chunk are not read: they may lie past the
+// end of the buffer's last row).
 template <int CH>
-__device__ __forceinline__ void stream_load(uint4 (&w)[CH], const void* p) {
+__device__ __forceinline__ void stream_load(uint4 (&w)[CH], const void* p, int chv) {
 #pragma unroll
-  for (int c = 0; c < CH; ++c) w[c] = __ldg(reinterpret_cast<const uint4*>(p) + c);
+  for (int c = 0; c < CH; ++c)
+    w[c] = (c == 0 || c < chv) ? __ldg(reinterpret_cast<const uint4*>(p) + c)
+                               : make_uint4(0u, 0u, 0u, 0u);
 }
 
-// Values of an outside lane's columns after unpacking the (clamped) edge
+// Values of a lane's columns outside the grid after unpacking its (clamped)
 // chunk: 0 under ZERO, the edge column under CLAMP; under COPY they never
-// reach an output that is kept, so they stay as loaded.
+// reach an output that is kept, so they stay as loaded.  `nin` = columns of a
+// partial chunk inside the grid.  (Grids with a partial last chunk run the
+// streaming kernel only under ZERO and COPY; under CLAMP every outside lane
+// is wholly outside, and its edge column is element 0 or V-1.)
 template <int V, typename TA>
-__device__ __forceinline__ void stream_fix_lane(TA (&d)[V], int where, int bnd) {
-  if (bnd == SSAM_BOUNDARY_ZERO) {
+__device__ __forceinline__ void stream_fix_lane(TA (&d)[V], int where, int nin, int bnd) {
+  if (bnd == SSAM_BOUNDARY_COPY) return;
+  if (where == kLanePartial) {
+#pragma unroll
+    for (int j = 1; j < V; ++j)
+      if (j >= nin) d[j] = TA(0);
+  } else if (bnd == SSAM_BOUNDARY_ZERO) {
 #pragma unroll
     for (int j = 0; j < V; ++j) d[j] = TA(0);
-  } else if (bnd == SSAM_BOUNDARY_CLAMP) {
+  } else {
     const TA e = where == kLaneLeft ? d[0] : d[V - 1];
 #pragma unroll
     for (int j = 0; j < V; ++j) d[j] = e;
   }
 }
 
-// Requirements (checked by the launcher, which hands other grids to the
-// windowed kernel): src/dst 16-byte aligned, pitch and width multiples of V.
-// Then every lane's columns are a whole 16-byte-aligned chunk either inside
-// the grid or outside it, and all loads are 16-byte loads of a clamped chunk.
-template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int SEG, int V_>
-__global__ void __launch_bounds__(256)
-stencil2d_stream_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int64_t W,
-                        int64_t H, int64_t pitch, int64_t y_begin, int64_t y_end, int bnd,
-                        CoefBlock<typename Traits<TS>::TA,
-                                  Stream2DCfg<TS, RL, RR, RT, RB, STAR, SEG, V_>::NC> cf) {
+// One warp's work: segments sg0, sg0 + sstride, ... (of SEGL rows from
+// y_begin; rows >= y_end are not written) of the strip whose first output
+// column is x_out0.  Shared by the grid kernel below and the persistent
+// batched kernel.  Requirements (checked by the launchers, which hand other
+// grids to the windowed kernel): src/dst 16-byte aligned, pitch a multiple
+// of V, and under CLAMP a width that is a multiple of V too.  Then every
+// lane's columns are one 16-byte-aligned chunk inside the grid, outside it,
+// or (width not a multiple of V) the row's last chunk, partly inside; all
+// loads are 16-byte loads of a clamped chunk (a partial chunk never leaves
+// its row's pitch, nor the 16-byte block of its last valid element).
+// PARTIAL: widths need not be a multiple of V (the batched kernel); without
+// it the launcher guarantees whole chunks and the partial-chunk code is left
+// out of the unrolled ring (it costs registers and instruction fetch).
+template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int SEG, int V_,
+          bool PARTIAL = false>
+__device__ __forceinline__ void stream2d_warp_segments(
+    const TS* __restrict__ src, TS* __restrict__ dst, int64_t W, int64_t H, int64_t pitch,
+    int64_t x_out0, int64_t y_begin, int64_t y_end, int sg0, int sstride, int bnd,
+    const CoefBlock<typename Traits<TS>::TA,
+                    Stream2DCfg<TS, RL, RR, RT, RB, STAR, SEG, V_>::NC>& cf) {
   using C = Stream2DCfg<TS, RL, RR, RT, RB, STAR, SEG, V_>;
   using TA = typename C::TA;
   constexpr int V = C::V, FW = C::FW, FH = C::FH, CH = C::CH, D = C::D, L = C::L,
                 PF = C::PF;
   constexpr int SEGL = C::SEGL;
   constexpr unsigned FULL = 0xffffffffu;
-  const int64_t warp_x = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int64_t x_out0 = warp_x * C::OUT_COLS;
-  if (x_out0 >= W) return;  // whole warp leaves together
   const int lane = threadIdx.x & 31;
   const int64_t x0 = x_out0 + (int64_t)(lane - C::HL) * V;
   const bool lane_stores = lane >= C::HL && lane < 32 - C::HR && x0 < W;
-  const int where = x0 < 0 ? kLaneLeft : (x0 >= W ? kLaneRight : kLaneIn);
-  // this lane's chunk, clamped into the grid
-  const int64_t xc = x0 < 0 ? 0 : (x0 >= W ? W - V : x0);
-  // warp-uniform: some lane of this warp lies outside the grid
+  const int where =
+      x0 < 0 ? kLaneLeft
+             : (x0 >= W ? kLaneRight : (PARTIAL && x0 + V > W ? kLanePartial : kLaneIn));
+  // this lane's chunk, clamped into the grid (the last chunk of a row)
+  const int64_t wlast = (W - 1) / V * V;
+  const int64_t xc = x0 < 0 ? 0 : (x0 > wlast ? wlast : x0);
+  // columns of that chunk inside the grid, and its 16-byte words holding any
+  const int nin = PARTIAL ? (int)(W - xc < V ? W - xc : V) : V;
+  const int chv = PARTIAL ? (nin * (int)sizeof(TS) + 15) / 16 : CH;
+  // warp-uniform: some lane of this warp lies outside the grid, or partly
   const bool edge_warp = x_out0 - (int64_t)C::HL * V < 0 || x_out0 + (32 - C::HL) * V > W;
   // columns of this lane that the COPY rule keeps at their input value
   const bool x_copy = bnd == SSAM_BOUNDARY_COPY && (x0 < RL || x0 + V > W - RR);
@@ -132,8 +158,10 @@ stencil2d_stream_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int64_
   const int h = (int)H;  // H, W < 2^31 (checked by the entry points)
   const bool fix_lane = edge_warp && where != kLaneIn;
   const bool copy = bnd == SSAM_BOUNDARY_COPY;
+  // rows RT .. h-RB-1 are not in the ring COPY keeps (none when h <= RT+RB)
+  const unsigned y_inner = h > RT + RB ? (unsigned)(h - RT - RB) : 0u;
 
-  for (int sg = blockIdx.y; sg < nseg; sg += gridDim.y) {
+  for (int sg = sg0; sg < nseg; sg += sstride) {
     const int ya = (int)y_begin + sg * SEGL;  // first output row of the segment
     // ring slot of grid row ya + k (k >= -RT) is (k + RT) % L
     uint4 raw[L][CH];
@@ -142,13 +170,15 @@ stencil2d_stream_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int64_
 #pragma unroll
     for (int k = 0; k < FH - 1 + D; ++k) {
       const int y = ya - RT + k;
-      stream_load<CH>(raw[k], (unsigned)y < (unsigned)h ? src + (int64_t)y * pitch + xc
-                                                        : (y < 0 ? row_top : row_bot));
+      stream_load<CH>(raw[k],
+                      (unsigned)y < (unsigned)h ? src + (int64_t)y * pitch + xc
+                                                : (y < 0 ? row_top : row_bot),
+                      chv);
     }
 #pragma unroll
     for (int k = 0; k < FH - 1; ++k) {
       stream_unpack<TS, V, CH>(val[k], raw[k]);
-      if (fix_lane) stream_fix_lane<V>(val[k], where, bnd);
+      if (fix_lane) stream_fix_lane<V>(val[k], where, nin, bnd);
     }
 
     // whole groups of L rows (rows past y_end are computed, not stored)
@@ -167,7 +197,7 @@ stencil2d_stream_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int64_
         {
           const int y = ya + i + RB + D;
           stream_load<CH>(raw[(u + FH - 1 + D) % L],
-                          (unsigned)y < (unsigned)h ? ldp : (y < 0 ? row_top : row_bot));
+                          (unsigned)y < (unsigned)h ? ldp : (y < 0 ? row_top : row_bot), chv);
           ldp += pitch;
         }
         // L2 prefetch PF rows further on, within the rows this segment reads
@@ -177,7 +207,7 @@ stencil2d_stream_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int64_
         pfp += pitch;
         // the row entering the reach
         stream_unpack<TS, V, CH>(val[(u + FH - 1) % L], raw[(u + FH - 1) % L]);
-        if (fix_lane) stream_fix_lane<V>(val[(u + FH - 1) % L], where, bnd);
+        if (fix_lane) stream_fix_lane<V>(val[(u + FH - 1) % L], where, nin, bnd);
 
         TA acc[V];
 #pragma unroll
@@ -255,19 +285,36 @@ stencil2d_stream_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int64_
           }
         }
         const int y = ya + i;
-        if (copy && (x_copy || (unsigned)(y - RT) >= (unsigned)(h - RT - RB))) {
-          const bool y_ring = (unsigned)(y - RT) >= (unsigned)(h - RT - RB);
+        if (copy && (x_copy || (unsigned)(y - RT) >= y_inner)) {
+          const bool y_ring = (unsigned)(y - RT) >= y_inner;
 #pragma unroll
           for (int j = 0; j < V; ++j) {
             const int64_t x = x0 + j;
             if (y_ring | (x < RL) | (x >= W - RR)) acc[j] = val[(u + RT) % L][j];
           }
         }
-        if (lane_stores && y < (int)y_end) store_vec<TS, V>(stp, acc);
+        if (lane_stores && y < (int)y_end) {
+          if (!PARTIAL || where == kLaneIn) store_vec<TS, V>(stp, acc);
+          else store_row_edge<TS, V>(stp - x0, x0, W, acc);  // the row's partial chunk
+        }
         stp += pitch;
       }
     }
   }
+}
+
+template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int SEG, int V_>
+__global__ void __launch_bounds__(256)
+stencil2d_stream_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int64_t W,
+                        int64_t H, int64_t pitch, int64_t y_begin, int64_t y_end, int bnd,
+                        CoefBlock<typename Traits<TS>::TA,
+                                  Stream2DCfg<TS, RL, RR, RT, RB, STAR, SEG, V_>::NC> cf) {
+  using C = Stream2DCfg<TS, RL, RR, RT, RB, STAR, SEG, V_>;
+  const int64_t warp_x = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int64_t x_out0 = warp_x * C::OUT_COLS;
+  if (x_out0 >= W) return;  // whole warp leaves together
+  stream2d_warp_segments<TS, RL, RR, RT, RB, STAR, SEG, V_>(
+      src, dst, W, H, pitch, x_out0, y_begin, y_end, (int)blockIdx.y, (int)gridDim.y, bnd, cf);
 }
 
 template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int SEG, int V_>

@@ -75,3 +75,65 @@ def test_batched_256_uneven_grids_config4(cuda):
     m = star_matrix(c, 1)
     want = oracle.conv2d(h0, m.astype(np.float32), "copy", steps=50)
     assert_rel_close(got[0].cpu().numpy(), want, magnitude2d(h0, m, "copy", 50), 5e-4, "g0")
+
+
+def _pitched(host, cuda, tdt=torch.float32):
+    """A grid whose rows start on 128-byte boundaries (pitch rounded up),
+    the layout that lets the persistent launch stream rows."""
+    h, w = host.shape
+    es = torch.empty((), dtype=tdt).element_size()
+    pitch = -(-w * es // 128) * 128 // es
+    base = torch.zeros(h, pitch, dtype=tdt, device=cuda)
+    view = base[:, :w]
+    view.copy_(torch.from_numpy(host).to(tdt))
+    return view
+
+
+@pytest.mark.parametrize("kind,r", [("star", 1), ("box", 2), ("box", 1), ("star", 2),
+                                    ("box", 3)])
+@pytest.mark.parametrize("steps", [1, 2, 7])
+@pytest.mark.parametrize("bnd", ["zero", "copy"])
+def test_batched_pitched_grids_stream_rows(cuda, kind, r, steps, bnd):
+    """Pitched rows: the persistent launch's single-step phases take the
+    row-streaming warp tiles (widths need not be a multiple of the strip's
+    chunk); results equal the oracle's and, bit for bit, the per-grid
+    launches', and nothing beyond each grid's width is written."""
+    hosts = _grids(14, 1, 260, hash((kind, r, steps, bnd)) % 2**31)
+    if kind == "star":
+        c = normalised((4 * r + 1,), r)
+        m = star_matrix(c, r)
+        shape = S.STAR
+    else:
+        m = normalised((2 * r + 1, 2 * r + 1), r)
+        c = m.ravel()
+        shape = S.BOX
+    srcs = [_pitched(h, cuda) for h in hosts]
+    dsts = [_pitched(np.full(h.shape, 0, np.float32), cuda) for h in hosts]
+    for d in dsts:
+        d._base.fill_(9.0)  # the pitch padding must keep this value
+    got = S.stencil2d_batched(srcs, c, r, shape, steps, bnd, dsts=dsts, persistent=True)
+    ref = S.stencil2d_batched(srcs, c, r, shape, steps, bnd, persistent=False)
+    S.device_status()
+    for h, a, b, d in zip(hosts, got, ref, dsts):
+        pad = d._base[:, h.shape[1]:]
+        assert bool((pad == 9.0).all()), "wrote past a grid's width"
+        a = a.cpu().numpy()
+        want = oracle.conv2d(h, m.astype(np.float32), bnd, steps=steps)
+        assert_rel_close(a, want, magnitude2d(h, m, bnd, steps), 1e-5 * steps, f"{h.shape}")
+        np.testing.assert_array_equal(a, b.cpu().numpy())
+
+
+@pytest.mark.parametrize("tdt,rel", [(torch.float64, 1e-12), (torch.bfloat16, 2.0**-8)])
+@pytest.mark.parametrize("bnd", ["copy", "clamp"])
+def test_batched_pitched_other_dtypes_and_clamp(cuda, tdt, rel, bnd):
+    steps = 1 if bnd == "clamp" else 5
+    hosts = _grids(9, 3, 150, 17)
+    c = normalised((5,), 1)
+    m = star_matrix(c, 1)
+    srcs = [_pitched(h, cuda, tdt) for h in hosts]
+    got = S.stencil2d_batched(srcs, c, 1, S.STAR, steps, bnd)
+    for s_, a in zip(srcs, got):
+        x = s_.double().cpu().numpy()
+        want = oracle.conv2d(x, m, bnd, steps=steps)
+        scale = np.maximum(np.abs(want), magnitude2d(x, m, bnd, steps))
+        assert_rel_close(a.double().cpu().numpy(), want, scale, rel * steps, f"{tdt} {bnd}")

@@ -87,21 +87,23 @@ def test_streaming_bf16_vs_fp64_oracle(cuda, tmp_path, kind, r, seg):
     assert_rel_close(got, want, scale, 2.0**-8 + 1e-5, f"bf16 {kind}{r}/seg{seg}")
 
 
-@pytest.mark.parametrize("h,w", [(40, 515), (1, 64), (2, 8), (133, 4)])
+@pytest.mark.parametrize("h,w", [(40, 515), (1, 64), (2, 8), (133, 4), (3, 64), (4, 8)])
 def test_streaming_pin_on_unaligned_and_tiny_grids(cuda, tmp_path, h, w):
     """Widths that are not a multiple of V go to the windowed kernel; tiny
     grids (one row, one strip, one chunk) stream with most lanes outside."""
     src = uniform((h, w), -1, 1, np.float32, h * 1000 + w)
-    c, m, shape, star = stencil("box", 1, 3)
-    force(tmp_path, np.float32, 1, star, w, h, 32)
-    try:
-        for bnd in ("zero", "copy", "clamp"):
-            got = S.stencil2d(torch.from_numpy(src).to(cuda), c, 1, shape,
-                              boundary=bnd).cpu().numpy()
-            want = oracle.conv2d(src, m.astype(np.float32), bnd)
-            assert_rel_close(got, want, magnitude2d(src, m, bnd), 1e-5, f"{h}x{w}/{bnd}")
-    finally:
-        S.autotune_clear()
+    for r in (1, 2):  # r = 2: heights up to 4 lie wholly in the ring COPY keeps
+        c, m, shape, star = stencil("box", r, 3)
+        force(tmp_path, np.float32, r, star, w, h, 32)
+        try:
+            for bnd in ("zero", "copy", "clamp"):
+                got = S.stencil2d(torch.from_numpy(src).to(cuda), c, r, shape,
+                                  boundary=bnd).cpu().numpy()
+                want = oracle.conv2d(src, m.astype(np.float32), bnd)
+                assert_rel_close(got, want, magnitude2d(src, m, bnd), 1e-5,
+                                 f"r{r} {h}x{w}/{bnd}")
+        finally:
+            S.autotune_clear()
 
 
 def test_streaming_rows_band(cuda, tmp_path):
@@ -122,3 +124,42 @@ def test_streaming_rows_band(cuda, tmp_path):
         S.autotune_clear()
     want = oracle.conv2d(src, m.astype(np.float32), "zero")
     assert_rel_close(got, want, magnitude2d(src, m, "zero"), 1e-5, "band")
+
+
+@pytest.mark.parametrize("dt", ["f32", "f64", "bf16"])
+@pytest.mark.parametrize("kind,r", [("star", 1), ("box", 2), ("star", 3), ("box", 3)])
+@pytest.mark.parametrize("w", [517, 6, 1, 33])
+@pytest.mark.parametrize("bnd", ["zero", "copy", "clamp"])
+def test_streaming_pitched_rows_with_a_partial_last_chunk(cuda, tmp_path, dt, kind, r, w, bnd):
+    """Rows 16-byte aligned (pitch a multiple of 32 elements) but widths that
+    are not a multiple of V: the row's last chunk is partly inside the grid
+    (loaded whole inside the row's pitch, its outside columns fixed by the
+    boundary rule, stored per element)."""
+    h = 77
+    tdt = {"f32": torch.float32, "f64": torch.float64, "bf16": torch.bfloat16}[dt]
+    pitch = -(-w // 32) * 32
+    base = torch.empty(h, pitch, dtype=tdt, device=cuda)
+    x32 = uniform((h, w), -1, 1, np.float32, w * 10 + r)
+    src = base[:, :w]
+    src.copy_(torch.from_numpy(x32).to(tdt))
+    c, m, shape, star = stencil(kind, r, 3 + r)
+    force(tmp_path, {"f32": np.float32, "f64": np.float64, "bf16": "bf16"}[dt], r, star, w, h, 32)
+    dbase = torch.full((h, pitch), 7.0, dtype=tdt, device=cuda)
+    dst = dbase[:, :w]
+    try:
+        S.stencil2d(src, c, r, shape, boundary=bnd, dst=dst)
+        got = dst.double().cpu().numpy()
+        pad = dbase[:, w:].double().cpu().numpy()
+    finally:
+        S.autotune_clear()
+    assert (pad == 7.0).all(), "wrote outside the grid's width"
+    ref_in = src.double().cpu().numpy()
+    want = oracle.conv2d(ref_in, m, bnd)
+    if dt == "bf16":
+        scale = np.maximum(np.abs(want), magnitude2d(ref_in, m, bnd))
+        assert_rel_close(got, want, scale, 2.0**-8 + 1e-5, f"{dt} {kind}{r} w{w} {bnd}")
+    else:
+        np_dt = np.float32 if dt == "f32" else np.float64
+        want = oracle.conv2d(ref_in.astype(np_dt), m.astype(np_dt), bnd)
+        rel = 1e-5 if dt == "f32" else 1e-12
+        assert_rel_close(got, want, magnitude2d(ref_in, m, bnd), rel, f"{dt} {kind}{r} w{w} {bnd}")
