@@ -326,6 +326,20 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
     // does my strip touch the x/y ring that COPY keeps?
     const bool ring_xy = w.boundary == SSAM_BOUNDARY_COPY &&
                          (x0 < R || x0 + V > nx - R || y0 < R || y0 + PY > ny - R);
+    // this thread's output rows at plane za (advanced by one plane per z), the
+    // rows inside the grid, and whether every row of the segment takes whole
+    // vector stores (alignment is the same for all of them when rows and
+    // planes are vector multiples)
+    constexpr int VB = V * (int)sizeof(TS);
+    constexpr int AL = VB >= 16 ? 16 : 8;
+    TS* outz = dst + (sg.b * nz + sg.za) * nxy + y0 * nx + x0;
+    unsigned row_ok = 0;
+#pragma unroll
+    for (int i = 0; i < PY; ++i)
+      if (y0 + i < ny && x0 < nx) row_ok |= 1u << i;
+    const bool vec_seg = x0 + V <= nx && (uintptr_t)outz % AL == 0 &&
+                         (nx * (int64_t)sizeof(TS)) % AL == 0 &&
+                         (nxy * (int64_t)sizeof(TS)) % AL == 0;
     // right-hand side rows, kept as raw 32-bit words: 2-byte types load plane
     // z+1 while plane z is computed (software pipelined across the z loop);
     // wider types load plane z at the top of its iteration (registers)
@@ -333,44 +347,50 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
     constexpr bool PIPE = sizeof(TS) == 2;
     uint32_t rawc[RHS ? PY : 1][RW];
     uint32_t rawn[(RHS && PIPE) ? PY : 1][RW];
-    auto load_rhs = [&](int64_t zz, uint32_t (&dst)[RHS ? PY : 1][RW]) {
+    const TS* rhz =
+        RHS ? (const TS*)w.rhs + (sg.b * nz + sg.za) * nxy + y0 * nx + x0 : nullptr;
+    const bool vec_rhs = RHS && x0 + V <= nx && (uintptr_t)rhz % AL == 0 &&
+                         (nx * (int64_t)sizeof(TS)) % AL == 0 &&
+                         (nxy * (int64_t)sizeof(TS)) % AL == 0;
+    // rows of plane za + zi
+    auto load_rhs = [&](int zi, uint32_t (&dstw)[RHS ? PY : 1][RW]) {
 #pragma unroll
       for (int i = 0; i < (RHS ? PY : 1); ++i) {
-        const int64_t y = y0 + i;
-        const TS* fp = (const TS*)w.rhs + (sg.b * nz + zz) * nxy + y * nx + x0;
-        if (y < ny && x0 + V <= nx && ((uintptr_t)fp % (RW >= 4 ? 16 : 8)) == 0) {
+        const TS* fp = rhz + (int64_t)zi * nxy + i * nx;
+        const bool in_row = (row_ok >> i) & 1u;
+        if (vec_rhs && in_row) {
           if constexpr (RW == 2) {
             const uint2 v = __ldg(reinterpret_cast<const uint2*>(fp));
-            dst[i][0] = v.x;
-            dst[i][1] = v.y;
+            dstw[i][0] = v.x;
+            dstw[i][1] = v.y;
           } else {
 #pragma unroll
             for (int c = 0; c < RW / 4; ++c) {
               const uint4 v = __ldg(reinterpret_cast<const uint4*>(fp) + c);
-              dst[i][4 * c] = v.x;
-              dst[i][4 * c + 1] = v.y;
-              dst[i][4 * c + 2] = v.z;
-              dst[i][4 * c + 3] = v.w;
+              dstw[i][4 * c] = v.x;
+              dstw[i][4 * c + 1] = v.y;
+              dstw[i][4 * c + 2] = v.z;
+              dstw[i][4 * c + 3] = v.w;
             }
           }
         } else {
           TS tmp[V];
 #pragma unroll
           for (int j = 0; j < V; ++j)
-            tmp[j] = (y < ny && x0 + j < nx) ? fp[j] : from_acc<TS>(TA(0));
-          memcpy(dst[i], tmp, sizeof(tmp));
+            tmp[j] = (in_row && x0 + j < nx) ? fp[j] : from_acc<TS>(TA(0));
+          memcpy(dstw[i], tmp, sizeof(tmp));
         }
       }
     };
-    if constexpr (RHS && PIPE) load_rhs(sg.za, rawc);
+    if constexpr (RHS && PIPE) load_rhs(0, rawc);
     for (int64_t z = sg.za; z < sg.zb; ++z) {
       // planes z-R .. z+R sit at ring positions n + (z - za) .. + 2R
       const uint32_t q0 = n + (uint32_t)(z - sg.za);
       if constexpr (RHS) {
         if constexpr (PIPE) {
-          if (z + 1 < sg.zb) load_rhs(z + 1, rawn);
+          if (z + 1 < sg.zb) load_rhs((int)(z + 1 - sg.za), rawn);
         } else {
-          load_rhs(z, rawc);
+          load_rhs((int)(z - sg.za), rawc);
         }
       }
       bool ok = true;
@@ -479,10 +499,7 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
 #pragma unroll
       for (int i = 0; i < PY; ++i) {
         const int64_t y = y0 + i;
-        if (y >= ny || x0 >= nx) continue;
-        const int64_t cell = (sg.b * nz + z) * nxy + y * nx + x0;
-        constexpr int VB = V * (int)sizeof(TS);
-        const bool vec = x0 + V <= nx && ((uintptr_t)(dst + cell) % (VB >= 16 ? 16 : 8)) == 0;
+        if (!((row_ok >> i) & 1u)) continue;
         TA o[V];
 #pragma unroll
         for (int j = 0; j < V; ++j) o[j] = acc[i][j];
@@ -499,8 +516,8 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
             if (zring || y < R || y >= ny - R || x < R || x >= nx - R) o[j] = center[i][j];
           }
         }
-        TS* outp = dst + cell;
-        if (vec) {
+        TS* outp = outz + i * nx;
+        if (vec_seg) {
           store_row<TS, V>(outp, o);
         } else {
 #pragma unroll
@@ -508,6 +525,7 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
             if (x0 + j < nx) outp[j] = from_acc<TS>(o[j]);
         }
       }
+      outz += nxy;
       if constexpr (RHS && PIPE) {
 #pragma unroll
         for (int i = 0; i < PY; ++i)

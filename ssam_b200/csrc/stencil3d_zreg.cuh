@@ -88,17 +88,37 @@ stencil3d_zreg_kernel(const __grid_constant__ CUtensorMap map, const TS* __restr
     // does my strip touch the x/y ring that COPY keeps?
     const bool ring_xy = w.boundary == SSAM_BOUNDARY_COPY &&
                          (x0 < R || x0 + V > nx - R || y0 < R || y0 + PY > ny - R);
+    // this thread's output rows at plane za (advanced by one plane per z), the
+    // rows inside the grid, and whether every row of the segment takes whole
+    // vector stores (alignment is the same for all of them when rows and
+    // planes are vector multiples)
+    constexpr int VB = V * (int)sizeof(TS);
+    constexpr int AL = VB >= 16 ? 16 : 8;
+    TS* outz = dst + (sg.b * nz + sg.za) * nxy + y0 * nx + x0;
+    unsigned row_ok = 0;
+#pragma unroll
+    for (int i = 0; i < PY; ++i)
+      if (y0 + i < ny && x0 < nx) row_ok |= 1u << i;
+    const bool vec_seg = x0 + V <= nx && (uintptr_t)outz % AL == 0 &&
+                         (nx * (int64_t)sizeof(TS)) % AL == 0 &&
+                         (nxy * (int64_t)sizeof(TS)) % AL == 0;
     // right-hand side rows as raw 32-bit words (as in stencil3d_kernel)
     constexpr int RW = V * (int)sizeof(TS) / 4;
     constexpr bool PIPE = sizeof(TS) == 2;
     uint32_t rawc[RHS ? PY : 1][RW];
     uint32_t rawn[(RHS && PIPE) ? PY : 1][RW];
-    auto load_rhs = [&](int64_t zz, uint32_t (&dstw)[RHS ? PY : 1][RW]) {
+    const TS* rhz =
+        RHS ? (const TS*)w.rhs + (sg.b * nz + sg.za) * nxy + y0 * nx + x0 : nullptr;
+    const bool vec_rhs = RHS && x0 + V <= nx && (uintptr_t)rhz % AL == 0 &&
+                         (nx * (int64_t)sizeof(TS)) % AL == 0 &&
+                         (nxy * (int64_t)sizeof(TS)) % AL == 0;
+    // rows of plane za + zi
+    auto load_rhs = [&](int zi, uint32_t (&dstw)[RHS ? PY : 1][RW]) {
 #pragma unroll
       for (int i = 0; i < (RHS ? PY : 1); ++i) {
-        const int64_t y = y0 + i;
-        const TS* fp = (const TS*)w.rhs + (sg.b * nz + zz) * nxy + y * nx + x0;
-        if (y < ny && x0 + V <= nx && ((uintptr_t)fp % (RW >= 4 ? 16 : 8)) == 0) {
+        const TS* fp = rhz + (int64_t)zi * nxy + i * nx;
+        const bool in_row = (row_ok >> i) & 1u;
+        if (vec_rhs && in_row) {
           if constexpr (RW == 2) {
             const uint2 v = __ldg(reinterpret_cast<const uint2*>(fp));
             dstw[i][0] = v.x;
@@ -117,12 +137,12 @@ stencil3d_zreg_kernel(const __grid_constant__ CUtensorMap map, const TS* __restr
           TS tmp[V];
 #pragma unroll
           for (int j = 0; j < V; ++j)
-            tmp[j] = (y < ny && x0 + j < nx) ? fp[j] : from_acc<TS>(TA(0));
+            tmp[j] = (in_row && x0 + j < nx) ? fp[j] : from_acc<TS>(TA(0));
           memcpy(dstw[i], tmp, sizeof(tmp));
         }
       }
     };
-    if constexpr (RHS && PIPE) load_rhs(sg.za, rawc);
+    if constexpr (RHS && PIPE) load_rhs(0, rawc);
 
     // register ring: plane p = za - R + k sits in zr[k % F]
     TA zr[F][PY][V];
@@ -155,9 +175,9 @@ stencil3d_zreg_kernel(const __grid_constant__ CUtensorMap map, const TS* __restr
         const uint32_t q0 = n + (uint32_t)zi;  // ring position of plane z-R
         if constexpr (RHS) {
           if constexpr (PIPE) {
-            if (zi + 1 < nzc) load_rhs(z + 1, rawn);
+            if (zi + 1 < nzc) load_rhs(zi + 1, rawn);
           } else {
-            load_rhs(z, rawc);
+            load_rhs(zi, rawc);
           }
         }
         // the plane entering the register ring: z+R
@@ -267,10 +287,7 @@ stencil3d_zreg_kernel(const __grid_constant__ CUtensorMap map, const TS* __restr
 #pragma unroll
         for (int i = 0; i < PY; ++i) {
           const int64_t y = y0 + i;
-          if (y >= ny || x0 >= nx) continue;
-          const int64_t cell = (sg.b * nz + z) * nxy + y * nx + x0;
-          constexpr int VB = V * (int)sizeof(TS);
-          const bool vec = x0 + V <= nx && ((uintptr_t)(dst + cell) % (VB >= 16 ? 16 : 8)) == 0;
+          if (!((row_ok >> i) & 1u)) continue;
           TA o[V];
 #pragma unroll
           for (int j = 0; j < V; ++j) o[j] = acc[i][j];
@@ -287,8 +304,8 @@ stencil3d_zreg_kernel(const __grid_constant__ CUtensorMap map, const TS* __restr
               if (zring || y < R || y >= ny - R || x < R || x >= nx - R) o[j] = zr[zc][i][j];
             }
           }
-          TS* outp = dst + cell;
-          if (vec) {
+          TS* outp = outz + i * nx;
+          if (vec_seg) {
             store_row<TS, V>(outp, o);
           } else {
 #pragma unroll
@@ -296,6 +313,7 @@ stencil3d_zreg_kernel(const __grid_constant__ CUtensorMap map, const TS* __restr
               if (x0 + j < nx) outp[j] = from_acc<TS>(o[j]);
           }
         }
+        outz += nxy;
         if constexpr (RHS && PIPE) {
 #pragma unroll
           for (int i = 0; i < PY; ++i)
