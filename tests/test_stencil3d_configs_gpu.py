@@ -55,7 +55,12 @@ def cube_for(shape, r):
     return cube / np.abs(cube).sum(), S.STAR3D
 
 
-@pytest.mark.parametrize("dt,shape,r,cfg", stencil_cases())
+def case_id(c):
+    dt, shape, r, (py, nw, s, zreg) = c
+    return f"{dt}-{'p19' if shape else 'star'}{r}-{py}x{nw}x{s}{'z' if zreg else ''}"
+
+
+@pytest.mark.parametrize("dt,shape,r,cfg", stencil_cases(), ids=[case_id(c) for c in stencil_cases()])
 @pytest.mark.parametrize("dims", [(40, 75, 200), (19, 33, 130)])
 @pytest.mark.parametrize("bnd", ["zero", "copy"])
 def test_every_3d_configuration_vs_oracle(cuda, tmp_path, dt, shape, r, cfg, dims, bnd):
@@ -86,7 +91,9 @@ def sweep_cases():
             if rhs]
 
 
-@pytest.mark.parametrize("dt,cfg", sweep_cases())
+@pytest.mark.parametrize("dt,cfg", sweep_cases(),
+                         ids=[f"{d}-{c[0]}x{c[1]}x{c[2]}{'z' if c[3] else ''}"
+                              for d, c in sweep_cases()])
 def test_every_jacobi_configuration_vs_oracle(cuda, tmp_path, dt, cfg):
     n, nb, sweeps = 24, 3, 2
     rel = {"f64": 1e-12, "f32": 1e-5, "bf16": 2.0**-8}[dt]
