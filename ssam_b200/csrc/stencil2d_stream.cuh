@@ -37,8 +37,8 @@ struct Stream2DCfg {
   static constexpr int OUT_COLS = OUT_LANES * V;
   static constexpr int CH = V * (int)sizeof(TS) / 16;  // 16-byte words per row
   // rows in flight ahead of the reach: 2 KB (FP32/16-bit) or 4 KB (FP64) a
-  // warp; one row for the 13-row reach, whose longer ring the compiler keeps
-  // in local memory
+  // warp (one row for reaches of 13 rows and more, whose longer ring the
+  // compiler would otherwise keep in local memory)
   static constexpr int D = FH >= 13 ? 1 : 4;
   static constexpr int L = FH + D;  // ring length = unroll factor
   // rows beyond the ones in flight that are prefetched into L2 (no registers
