@@ -117,15 +117,16 @@ def taps(spec) -> int:
 
 def cube3d(spec) -> np.ndarray:
     """The reference's own 3D coefficients (_F<z><y><x> defines, read from the
-    committed tests/golden/coefficients.json), scaled to sum 1 so that 100
-    steps stay bounded."""
+    committed tests/golden/coefficients.json), scaled so that their absolute
+    values sum to 1: 100 steps stay bounded (the 19-point operator has
+    coefficients of both signs)."""
     with open(os.path.join(ROOT, "tests", "golden", "coefficients.json")) as f:
         c = json.load(f)["coeffs3d"][spec["gold"]]
     r = spec["r"]
     cube = np.zeros((2 * r + 1,) * 3)
     for k, v in c.items():
         cube[int(k[0]), int(k[1]), int(k[2])] = v
-    return cube / cube.sum()
+    return cube / np.abs(cube).sum()
 
 
 def coefficients(spec):
@@ -1006,6 +1007,19 @@ def run_ssam(args, spec, name):
     alg_bytes = 2 * n ** len(dims) * es * launches_per_step
     achieved = alg_bytes / (avg_launch_ms / 1e3) / 1e9
     traffic = load_traffic(name)
+    # the binding roof of one launch: HBM (bytes above) or the FP32 / FP64
+    # FMA pipes, 2*taps-1 flop per cell and fused step; the FMA peak is the
+    # nominal SM count x FMA lanes x 2 x maximum SM clock (no measured figure
+    # exists for the non-tensor pipes)
+    per_launch_s = avg_launch_ms / 1e3 / (1 if graph is not None else launches_per_step)
+    flops_per_launch = ((2 * taps(spec) - 1) * n ** len(dims) * spec["steps"]
+                        / launches_per_step)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    max_mhz = (clk or {}).get("sm_max_mhz") or 1965.0
+    fma_lanes = 64 if spec["dtype"] == "f64" else 128
+    fma_peak = sms * fma_lanes * 2 * max_mhz * 1e6 / 1e12  # TFLOP/s
+    fma_bound = flops_per_launch / (fma_peak * 1e12) > (alg_bytes / launches_per_step) / (peak * 1e9)
+    fma_achieved = flops_per_launch / per_launch_s / 1e12
 
     # reduced-precision runs: max / RMS error of the last call's result
     # against the same call in FP64 on the same stored inputs (the FP64
@@ -1082,11 +1096,22 @@ def run_ssam(args, spec, name):
                                    else "K calls",
                        "tuned": tuned},
             "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak,
-                         "peak_source": peak_kind,
-                         "traffic": traffic,
-                         "algorithmic_bytes_per_launch": alg_bytes / launches_per_step},
+            "roofline": ({"bound": "fma", "achieved": fma_achieved, "peak": fma_peak,
+                          "unit": "TFLOP/s", "frac": fma_achieved / fma_peak,
+                          "peak_source": f"nominal: {sms} SMs x {fma_lanes} FMA lanes x 2 x "
+                                         f"{max_mhz:.0f} MHz",
+                          "traffic": traffic,
+                          "algorithmic_flops_per_launch": flops_per_launch,
+                          "hbm": {"achieved": achieved, "peak": peak, "unit": "GB/s",
+                                  "frac": achieved / peak, "peak_source": peak_kind}}
+                         if fma_bound else
+                         {"bound": "hbm", "achieved": achieved, "peak": peak,
+                          "unit": "GB/s", "frac": achieved / peak,
+                          "peak_source": peak_kind,
+                          "traffic": traffic,
+                          "algorithmic_bytes_per_launch": alg_bytes / launches_per_step,
+                          "fma": {"achieved": fma_achieved, "peak": fma_peak,
+                                  "unit": "TFLOP/s", "frac": fma_achieved / fma_peak}}),
             "clocks": clk,
             "e2e": e2e,
             "cpu_baseline": cpu,
