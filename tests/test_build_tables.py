@@ -1,0 +1,65 @@
+"""The compiled-configuration tables of ssam_b200/build.py, checked on the
+CPU: every 3D configuration fits one SM's shared memory and has the ring
+depth its kernel needs, defaults are unique per group, and the 2D tables
+cover what the entry points and the autotuner look up."""
+from collections import Counter
+
+import pytest
+
+from ssam_b200.build import instances, instances_3d, stream_instances
+
+ES = {"f32": 4, "f64": 8, "bf16": 2, "f16": 2}
+SMEM_PER_CTA = 227 * 1024
+
+
+def smem_3d(dt, shape, r, py, nw, s):
+    """Dynamic shared memory of a 3D CTA as the launcher requests it
+    (Stencil3DCfg::SMEM): S slots of (128 + 2*HX) x (NW*PY + 2*RYM) elements
+    rounded to 128 bytes, two mbarriers per slot, 128 bytes of alignment."""
+    es = ES[dt]
+    hx = 16 // es
+    xw = 128 + 2 * hx
+    rym = 1 if shape == 1 else r
+    yw = nw * py + 2 * rym
+    slot = (xw * yw * es + 127) // 128 * 128
+    return s * slot + 2 * s * 8 + 128
+
+
+@pytest.mark.parametrize("inst", instances_3d(), ids=lambda c: "-".join(map(str, c)))
+def test_3d_configuration_fits_and_has_its_ring(inst):
+    dt, shape, r, py, nw, s, rhs, dflt, zreg = inst
+    assert smem_3d(dt, shape, r, py, nw, s) <= SMEM_PER_CTA
+    assert 32 * (nw + 1) <= 1024
+    rh = 1 if shape == 1 else 0  # planes read for halos: z-RH .. z+RH
+    need = r + rh + 2 if zreg else 2 * r + 2
+    assert s >= need, f"ring of {s} slots, kernel needs {need}"
+    if rhs:
+        assert shape == 0 and r == 1  # the Jacobi sweep is the 7-point star
+
+
+def test_3d_groups_have_exactly_one_default():
+    groups = Counter((dt, shape, r, rhs) for (dt, shape, r, _, _, _, rhs, dflt, _)
+                     in instances_3d() if dflt)
+    every = {(dt, shape, r, rhs) for (dt, shape, r, _, _, _, rhs, _, _) in instances_3d()}
+    assert set(groups) == every and all(v == 1 for v in groups.values())
+
+
+def test_3d_table_covers_the_entry_points():
+    have = {(dt, shape, r, rhs) for (dt, shape, r, _, _, _, rhs, _, _) in instances_3d()}
+    for dt in ("f32", "f64", "bf16", "f16"):
+        for shape, r in ((0, 1), (0, 2), (1, 1)):
+            assert (dt, shape, r, False) in have
+    for dt in ("f32", "f64", "bf16"):  # Poisson sweep storage types
+        assert (dt, 0, 1, True) in have
+
+
+def test_2d_tables():
+    win = set(instances())
+    # the windowed fallback every streaming launcher hands unaligned grids to
+    for (dt, star, r, seg, v) in stream_instances():
+        assert seg >= 32 and (dt, star, r, r, 8, 1, v) in win
+    # single-step kernels for every star r <= 6 and box r <= 5 in every type
+    for dt in ("f32", "f64", "bf16", "f16"):
+        for star, rmax in ((1, 6), (0, 5)):
+            for r in range(1, rmax + 1):
+                assert any(k[:4] == (dt, star, r, r) and k[5] == 1 for k in win)
