@@ -110,6 +110,20 @@ def instances_3d():
     return out
 
 
+def rowloop_instances():
+    """(dtype, rl, rr, V) of every compiled row-loop 2D kernel (square filters
+    of width FW = rl + rr + 1 >= 7: box r = 3..5 and the wider correlations;
+    registered with P = 1)."""
+    out = []
+    for dt, vs in (("f32", (4, 8)), ("f64", (4,))):
+        for f in range(7, 29):
+            rl, rr = f // 2, f - 1 - f // 2
+            for v in vs:
+                if (rl + v - 1) // v + (rr + v - 1) // v <= 30:
+                    out.append((dt, rl, rr, v))
+    return out
+
+
 def stream_instances():
     """(dtype, star, r, SEG, V) of every compiled row-streaming 2D kernel
     (one step per launch; a warp walks SEG output rows), registered with
@@ -167,6 +181,25 @@ def _gen_units(chunk: int = 6):
                     f"static Register3D<{DTYPES[dt]}, {sh}, {r}, {py}, {nw}, {s}, "
                     f"{'true' if rhs else 'false'}, {'true' if dflt else 'false'}, "
                     f"{'true' if zreg else 'false'}> reg3_{tag};")
+            lines.append("}  // namespace ssam")
+            text = "\n".join(lines) + "\n"
+            path = os.path.join(BUILD, "gen", name)
+            if not os.path.exists(path) or open(path).read() != text:
+                with open(path, "w") as f:
+                    f.write(text)
+            units.append(path)
+    by_dt = {}
+    for inst in rowloop_instances():
+        by_dt.setdefault(inst[0], []).append(inst)
+    for dt, lst in by_dt.items():
+        for c in range(0, len(lst), chunk):
+            part = lst[c:c + chunk]
+            name = f"inst2dr_{dt}_{c // chunk:02d}.cu"
+            lines = ["// generated by ssam_b200/build.py -- do not edit",
+                     '#include "../../csrc/stencil2d_rowloop.cuh"', "namespace ssam {"]
+            for (_, rl, rr, v) in part:
+                lines.append(f"static RegisterRowLoop2D<{DTYPES[dt]}, {rl}, {rr}, {rl}, {rr}, {v}> "
+                             f"regr_{rl}_{rr}_{v};")
             lines.append("}  // namespace ssam")
             text = "\n".join(lines) + "\n"
             path = os.path.join(BUILD, "gen", name)
