@@ -5,16 +5,16 @@
 // row it keeps: for a 21 x 21 correlation and 4 rows a thread that is over
 // ten thousand FMAs of straight-line code, far more than the instruction
 // cache holds, and the kernel stalls on instruction fetch.  Here a warp keeps
-// one output row at a time and walks the filter rows in a loop that is not
-// unrolled: per filter row it loads the input row for its strip (V columns a
-// lane, halo lanes beyond both sides, 16-byte loads), reads that filter row's
-// coefficients, and forms the own-column products and the partial sums for
-// the lanes downstream -- the same products in the same order as the
-// windowed tile.  The partial sums travel by shuffle once per output row, after
-// the last filter row (SSAM's systolic exchange).  The input rows of
-// neighbouring output rows are re-read from L1/L2, not DRAM.  Registered in
-// the kernel table with P = 1, which the autotuner times against the other
-// tiles.
+// one output row at a time and walks the filter rows in a loop unrolled only
+// by two: per filter row it loads the input row for its strip (V columns a
+// lane, halo lanes beyond both sides, 16-byte loads; the next row's load is
+// issued before this row's products), reads that filter row's coefficients,
+// and forms the own-column products and the partial sums for the lanes
+// downstream -- the same products in the same order as the windowed tile.
+// The partial sums travel by shuffle once per output row, after the last
+// filter row (SSAM's systolic exchange).  The input rows of neighbouring
+// output rows are re-read from L1/L2, not DRAM.  Registered in the kernel
+// table with P = 1, which the autotuner times against the other tiles.
 #pragma once
 
 #include "stencil2d.cuh"
@@ -72,25 +72,27 @@ stencil2d_rowloop_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int64
 #pragma unroll
       for (int q = 0; q < (RR > 0 ? RR : 1); ++q) pl[q] = TA(0);
 
-#pragma unroll 1
-      for (int fy = 0; fy < C::FH; ++fy) {
-        // input row y + dy (dy = fy - RT), with the boundary rule
+      // input row y + fy - RT with the boundary rule (ZERO: zeros outside)
+      auto load = [&](int fy, TA (&d)[V]) {
         int64_t yy = y + fy - RT;
         const bool y_out = yy < 0 || yy >= H;
-        if (y_out && bnd == SSAM_BOUNDARY_ZERO) continue;  // warp-uniform: adds zeros
         yy = yy < 0 ? 0 : (yy >= H ? H - 1 : yy);
         const TS* row = src + yy * pitch;
-        TA d[V];
-        if (row_vec) {
+        if (y_out && bnd == SSAM_BOUNDARY_ZERO) {
+#pragma unroll
+          for (int j = 0; j < V; ++j) d[j] = TA(0);
+        } else if (row_vec) {
           load_vec<TS, V>(d, row + x0);
         } else {
           load_row_edge<TS, V>(d, row, x0, W, bnd);
         }
-        // this filter row's coefficients (a runtime row of the constant block)
+      };
+      // one filter row's products: own columns, then the partial sums for
+      // the lanes to the right (virtual column V+q) and left (-1-q)
+      auto compute = [&](int fy, const TA (&d)[V]) {
         TA w[FW];
 #pragma unroll
         for (int dx = 0; dx < FW; ++dx) w[dx] = cf.c[fy * FW + dx];
-        // own columns
 #pragma unroll
         for (int dx = -RL; dx <= RR; ++dx) {
 #pragma unroll
@@ -99,8 +101,6 @@ stencil2d_rowloop_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int64
             acc[j] = fma(w[dx + RL], d[j + dx], acc[j]);
           }
         }
-        // partial sums for the lanes to the right (virtual column V+q) and
-        // to the left (virtual column -1-q)
         if constexpr (RL > 0) {
 #pragma unroll
           for (int q = 0; q < RL; ++q) {
@@ -123,6 +123,17 @@ stencil2d_rowloop_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int64
             }
           }
         }
+      };
+      // two rows in flight: the next row's load is issued before the
+      // current row's products (ping-pong between two register rows)
+      TA da[V], db[V];
+      load(0, da);
+#pragma unroll 1
+      for (int fy = 0; fy < C::FH; fy += 2) {
+        if (fy + 1 < C::FH) load(fy + 1, db);
+        compute(fy, da);
+        if (fy + 2 < C::FH) load(fy + 2, da);
+        if (fy + 1 < C::FH) compute(fy + 1, db);
       }
       // systolic exchange of the partial sums (a chain when a reach exceeds V)
       if constexpr (RL > 0) {
