@@ -124,6 +124,19 @@ def rowloop_instances():
     return out
 
 
+def stream_t_instances():
+    """(dtype, star, r, SEG, V, T) of every compiled row-streaming kernel with
+    T fused steps (r = 1: T = 2, 4; r = 2: T = 2), registered with P = SEG."""
+    out = []
+    for dt in ("f32", "f64", "bf16"):
+        v = 8 if dt == "bf16" else 4
+        for star in (1, 0):
+            for r, ts in ((1, (2, 4)), (2, (2,))):
+                for t in ts:
+                    out.append((dt, star, r, 64, v, t))
+    return out
+
+
 def stream_instances():
     """(dtype, star, r, SEG, V) of every compiled row-streaming 2D kernel
     (one step per launch; a warp walks SEG output rows), registered with
@@ -200,6 +213,27 @@ def _gen_units(chunk: int = 6):
             for (_, rl, rr, v) in part:
                 lines.append(f"static RegisterRowLoop2D<{DTYPES[dt]}, {rl}, {rr}, {rl}, {rr}, {v}> "
                              f"regr_{rl}_{rr}_{v};")
+            lines.append("}  // namespace ssam")
+            text = "\n".join(lines) + "\n"
+            path = os.path.join(BUILD, "gen", name)
+            if not os.path.exists(path) or open(path).read() != text:
+                with open(path, "w") as f:
+                    f.write(text)
+            units.append(path)
+    by_dt = {}
+    for inst in stream_t_instances():
+        by_dt.setdefault(inst[0], []).append(inst)
+    for dt, lst in by_dt.items():
+        for c in range(0, len(lst), 3):
+            part = lst[c:c + 3]
+            name = f"inst2dt_{dt}_{c // 3:02d}.cu"
+            lines = ["// generated by ssam_b200/build.py -- do not edit",
+                     '#include "../../csrc/stencil2d_stream_t.cuh"', "namespace ssam {"]
+            for (_, star, r, seg, v, t) in part:
+                lines.append(
+                    f"static RegisterStreamT2D<{DTYPES[dt]}, {r}, {r}, {r}, {r}, "
+                    f"{'true' if star else 'false'}, {seg}, {v}, {t}> "
+                    f"regt_{'s' if star else 'b'}_{r}_{t};")
             lines.append("}  // namespace ssam")
             text = "\n".join(lines) + "\n"
             path = os.path.join(BUILD, "gen", name)

@@ -63,3 +63,13 @@ def test_2d_tables():
         for star, rmax in ((1, 6), (0, 5)):
             for r in range(1, rmax + 1):
                 assert any(k[:4] == (dt, star, r, r) and k[5] == 1 for k in win)
+
+
+def test_fused_streaming_kernels_have_windowed_fallbacks():
+    """Grids the fused-step streaming launcher cannot take go to the windowed
+    kernel of the same stencil and depth (P = 8)."""
+    from ssam_b200.build import stream_t_instances
+    win = set(instances())
+    for (dt, star, r, seg, v, t) in stream_t_instances():
+        assert seg >= 32 and t >= 2
+        assert (dt, star, r, r, 8, t, v) in win
