@@ -94,7 +94,7 @@ CNN_WEIGHTS = os.path.join(ROOT, "ssam_b200", "data", "poisson_cnn_n128.bin")
 # sweeps between two FP64 residuals and the sweep damping of each arm
 POISSON_ARMS = {
     "plain": dict(sweep_dtype="f32", sweeps_per_correction=2000, omega=1.0),
-    "learned": dict(sweep_dtype="bf16", sweeps_per_correction=160, omega=0.8, cnn_smoothing=4),
+    "learned": dict(sweep_dtype="bf16", sweeps_per_correction=250, omega=0.8, cnn_smoothing=2),
 }
 # FP32-sweep defect-correction sweeps the plain arm needs for the 8 x 128^3
 # benchmark problem to reach 1e-5 (measured on a B200; the CPU reference arm

@@ -89,8 +89,8 @@ def test_trained_network_beats_the_plain_method(cuda):
     net = S.WarmStartCNN(n, nb)
     net.load(os.path.join(os.path.dirname(S.__file__), "data", "poisson_cnn_n128.bin"))
     arms = {"plain": dict(sweep_dtype="f32", sweeps_per_correction=2000, omega=1.0),
-            "learned": dict(sweep_dtype="bf16", sweeps_per_correction=160, omega=0.8,
-                            cnn_smoothing=4, cnn=net)}
+            "learned": dict(sweep_dtype="bf16", sweeps_per_correction=250, omega=0.8,
+                            cnn_smoothing=2, cnn=net)}
     out = {}
     for name, kw in arms.items():
         u = torch.zeros_like(f)
