@@ -2,10 +2,12 @@
 //
 // Drop-in for the reference's convolution program (ssai-2dconv/conv2D.cu:
 // 175-246: data type in argv[1], square grid size in argv[2] (default 8192),
-// square filter size 2..28 in argv[3] (default 3)).  Seeds the grid and the
-// filter, runs ssam_conv2d on the GPU (zero padding, offsets x + m - fw/2 and
-// y + n - fh/2 like the reference), prints the kernel time and GCells/s, and
-// checks 4096 sampled cells against a direct evaluation in double.
+// square filter size 2..28 in argv[3] (default 3)).  Reads the reference's
+// 8-bit input image ../data/Lena<size>x<size>.raw when it exists (else seeds
+// the grid), seeds the filter, runs ssam_conv2d on the GPU (zero padding,
+// offsets x + m - fw/2 and y + n - fh/2 like the reference), prints the kernel
+// time and GCells/s, and checks 4096 sampled cells against a direct
+// evaluation in double.
 #include "ssai_cli.h"
 
 namespace {
@@ -21,7 +23,17 @@ int run(int argc, char** argv) {
   }
   const int64_t W = size, H = size;
   const std::vector<double> w = ssai::coefficients((size_t)fsize * fsize, 13);
-  const std::vector<T> in = ssai::uniform<T>((size_t)W * H, 7);
+  // the reference's input image when it is there (conv2D.cu:88-104), else
+  // seeded data
+  std::vector<T> in;
+  char path[256];
+  snprintf(path, sizeof path, "../data/Lena%dx%d.raw", size, size);
+  if (ssai::load_raw_uchar<T>(path, (size_t)W * H, &in)) {
+    printf("Load success : %s\n", path);
+  } else {
+    printf("Load failed : %s, generate random data\n", path);
+    in = ssai::uniform<T>((size_t)W * H, 7);
+  }
   ssai::DeviceRun<T> dev(in);
   auto call = [&] {
     ssai::check(ssam_conv2d(dev.src, dev.dst, W, W, H, ssai::dtype<T>(), w.data(), fsize, fsize,

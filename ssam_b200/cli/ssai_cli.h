@@ -57,6 +57,22 @@ std::vector<T> uniform(size_t count, uint64_t seed) {
   return v;
 }
 
+// A raw 8-bit image of `count` pixels (the reference conv driver's
+// ../data/Lena<W>x<H>.raw, read by DataT::Load_uchar, ssai-2dconv/common.h:
+// 151-178) as values of T; false when the file is missing or short.
+template <typename T>
+bool load_raw_uchar(const char* path, size_t count, std::vector<T>* out) {
+  FILE* f = fopen(path, "rb");
+  if (!f) return false;
+  std::vector<unsigned char> px(count);
+  const size_t got = fread(px.data(), 1, count, f);
+  fclose(f);
+  if (got != count) return false;
+  out->resize(count);
+  for (size_t i = 0; i < count; ++i) (*out)[i] = (T)px[i];
+  return true;
+}
+
 // Device copy of a host vector, the result buffer and a timed launch.
 template <typename T>
 struct DeviceRun {

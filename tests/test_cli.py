@@ -10,9 +10,9 @@ BIN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), 
                    "bin")
 
 
-def run(exe, *args, timeout=300):
+def run(exe, *args, timeout=300, cwd=None):
     return subprocess.run([os.path.join(BIN, exe), *map(str, args)], capture_output=True,
-                          text=True, timeout=timeout)
+                          text=True, timeout=timeout, cwd=cwd)
 
 
 @pytest.mark.parametrize("exe", ["ssai-2dstencil", "ssai-2dconv", "ssai-3dstencil"])
@@ -56,3 +56,21 @@ def test_3dstencil_names(cuda, name, dtype, n, it):
     r = run("ssai-3dstencil", name, dtype, n, it)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "RMS Error" in r.stdout
+
+
+@pytest.mark.gpu
+def test_2dconv_reads_the_reference_raw_image(cuda, tmp_path):
+    """With ../data/Lena<N>x<N>.raw beside the working directory (the
+    reference driver's input, 8-bit pixels) the program convolves that image
+    and its sampled check still holds; without it, seeded data."""
+    import numpy as np
+    n = 256
+    (tmp_path / "data").mkdir()
+    (tmp_path / "run").mkdir()
+    img = (np.arange(n * n) * 37 % 251).astype(np.uint8)
+    (tmp_path / "data" / f"Lena{n}x{n}.raw").write_bytes(img.tobytes())
+    r = run("ssai-2dconv", "float", n, 5, cwd=str(tmp_path / "run"))
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert f"Load success : ../data/Lena{n}x{n}.raw" in r.stdout
+    r = run("ssai-2dconv", "float", 128, 5, cwd=str(tmp_path / "run"))
+    assert r.returncode == 0 and "Load failed" in r.stdout
