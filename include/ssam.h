@@ -263,10 +263,11 @@ SSAM_API int ssam_autotune_stencil2d(const void* src, void* dst, int64_t width,
 /* What the 3D autotuner chose for one stencil and grid size. */
 typedef struct ssam_tune3d_report {
   int rows_per_warp;  /* PY: rows of the column tile each consumer warp computes */
-  int consumer_warps; /* NW: consumer warps per CTA; the tile is 128 x NW*PY cells */
+  int consumer_warps; /* NW: consumer warps per CTA; the tile is 32*V x NW*PY cells */
   int ring_slots;     /* S: z-planes of the tile staged in shared memory */
   int registers_z;    /* 1: each thread keeps its own cells of the 2R+1 planes in
                          registers (shared memory carries the halos only) */
+  int columns_per_thread; /* V: the tile is 32*V columns wide */
   int candidates;     /* configurations timed */
   double ms_per_step; /* best measured time of one launch (ms) */
 } ssam_tune3d_report;

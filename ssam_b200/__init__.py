@@ -384,7 +384,7 @@ class Tune3DReport(ctypes.Structure):
     """``ssam_tune3d_report``."""
     _fields_ = [("rows_per_warp", ctypes.c_int), ("consumer_warps", ctypes.c_int),
                 ("ring_slots", ctypes.c_int), ("registers_z", ctypes.c_int),
-                ("candidates", ctypes.c_int),
+                ("columns_per_thread", ctypes.c_int), ("candidates", ctypes.c_int),
                 ("ms_per_step", ctypes.c_double)]
 
     def as_dict(self):

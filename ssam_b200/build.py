@@ -74,24 +74,29 @@ def instances():
 
 
 def instances_3d():
-    """(dtype, shape, r, PY, NW, S, rhs, default, zreg) of every compiled 3D
-    configuration: shape 0 = star (r = 1: 7-pt, r = 2: 13-pt), 1 = the
+    """(dtype, shape, r, PY, NW, S, rhs, default, zreg, V) of every compiled
+    3D configuration: shape 0 = star (r = 1: 7-pt, r = 2: 13-pt), 1 = the
     19-point Poisson operator; rhs = the Jacobi-sweep form with a
     right-hand-side term; zreg = the kernel that keeps each thread's own
-    cells in a register ring along z (stencil3d_zreg.cuh; "z" below).  The
-    first of each group is the default; the 3D autotuner times them all."""
+    cells in a register ring along z (stencil3d_zreg.cuh; "z" below); V =
+    columns a thread ("z8" / "c8" below: V = 8, a 256-column tile staged as
+    two TMA boxes; else 4).  The first of each group is the default; the 3D
+    autotuner times them all."""
     cfg = {
         "f32": {(0, 1): [(4, 8, 6), (4, 4, 8), (2, 16, 6), (4, 16, 5), (8, 8, 5),
-                         (2, 16, 4, "z"), (2, 8, 4, "z"), (2, 16, 8, "z"), (2, 8, 8, "z")],
+                         (2, 16, 4, "z"), (2, 8, 4, "z"), (2, 16, 8, "z"), (2, 8, 8, "z"),
+                         (2, 8, 4, "z8"), (2, 8, 8, "z8"), (4, 8, 6, "c8")],
                 (0, 2): [(4, 4, 8), (4, 8, 6), (2, 8, 6), (2, 16, 6), (4, 12, 6), (4, 12, 8),
-                         (2, 12, 4, "z"), (2, 16, 4, "z"), (2, 16, 8, "z"), (2, 12, 8, "z")],
+                         (2, 12, 4, "z"), (2, 16, 4, "z"), (2, 16, 8, "z"), (2, 12, 8, "z"),
+                         (2, 8, 4, "z8"), (2, 8, 8, "z8"), (4, 4, 8, "c8")],
                 (1, 1): [(4, 8, 6), (4, 4, 8), (2, 16, 6), (4, 16, 5), (4, 8, 8),
                          (2, 16, 4, "z"), (2, 8, 4, "z"), (2, 16, 8, "z")],
                 "rhs": [(4, 8, 6), (4, 4, 8), (2, 16, 6), (4, 16, 5),
                         (2, 16, 4, "z"), (2, 8, 4, "z"), (2, 16, 8, "z"), (2, 8, 8, "z")]},
         "bf16": {(0, 1): [(4, 8, 6), (2, 16, 6), (4, 16, 6), (8, 8, 6), (2, 16, 4, "z"),
-                          (2, 16, 8, "z")],
-                 (0, 2): [(4, 4, 8), (4, 8, 6), (2, 16, 6), (2, 12, 4, "z"), (2, 16, 8, "z")],
+                          (2, 16, 8, "z"), (2, 8, 4, "z8"), (4, 8, 6, "c8")],
+                 (0, 2): [(4, 4, 8), (4, 8, 6), (2, 16, 6), (2, 12, 4, "z"), (2, 16, 8, "z"),
+                          (2, 8, 4, "z8"), (2, 8, 8, "z8"), (4, 4, 8, "c8")],
                  (1, 1): [(4, 8, 6), (2, 16, 6), (4, 16, 6), (2, 16, 4, "z"), (2, 16, 8, "z")],
                  "rhs": [(4, 8, 6), (2, 16, 6), (4, 16, 6), (2, 16, 4, "z"), (2, 8, 4, "z"),
                          (2, 16, 8, "z")]},
@@ -106,7 +111,9 @@ def instances_3d():
         for key, lst in groups.items():
             shape, r, rhs = (0, 1, True) if key == "rhs" else (key[0], key[1], False)
             for i, c in enumerate(lst):
-                out.append((dt, shape, r, c[0], c[1], c[2], rhs, i == 0, len(c) > 3))
+                tag = c[3] if len(c) > 3 else ""
+                out.append((dt, shape, r, c[0], c[1], c[2], rhs, i == 0, tag.startswith("z"),
+                            8 if tag.endswith("8") else 4))
     return out
 
 
@@ -187,13 +194,13 @@ def _gen_units(chunk: int = 6):
             name = f"inst3d_{dt}_{c // 3:02d}.cu"
             lines = ["// generated by ssam_b200/build.py -- do not edit",
                      '#include "../../csrc/stencil3d_launch.cuh"', "namespace ssam {"]
-            for (_, shape, r, py, nw, s, rhs, dflt, zreg) in part:
+            for (_, shape, r, py, nw, s, rhs, dflt, zreg, v) in part:
                 sh = "SH3_POISSON19" if shape else "SH3_STAR"
-                tag = f"{shape}_{r}_{py}_{nw}_{s}_{int(rhs)}_{int(zreg)}"
+                tag = f"{shape}_{r}_{py}_{nw}_{s}_{int(rhs)}_{int(zreg)}_{v}"
                 lines.append(
                     f"static Register3D<{DTYPES[dt]}, {sh}, {r}, {py}, {nw}, {s}, "
                     f"{'true' if rhs else 'false'}, {'true' if dflt else 'false'}, "
-                    f"{'true' if zreg else 'false'}> reg3_{tag};")
+                    f"{'true' if zreg else 'false'}, {v}> reg3_{tag};")
             lines.append("}  // namespace ssam")
             text = "\n".join(lines) + "\n"
             path = os.path.join(BUILD, "gen", name)

@@ -269,8 +269,8 @@ extern "C" int ssam_autotune_save(const char* path) {
   }
   tune3d_for_each(
       [](const int* k, const int* v, void* u) {
-        fprintf((FILE*)u, "choice3d %d %d %d %d %d %d %d %d %d %d %d\n", k[0], k[1], k[2],
-                k[3], k[4], k[5], k[6], v[0], v[1], v[2], v[3]);
+        fprintf((FILE*)u, "choice3d %d %d %d %d %d %d %d %d %d %d %d %d\n", k[0], k[1], k[2],
+                k[3], k[4], k[5], k[6], v[0], v[1], v[2], v[3], v[4]);
       },
       f);
   fclose(f);
@@ -286,16 +286,20 @@ extern "C" int ssam_autotune_load(const char* path) {
   int bad = 0;
   std::lock_guard<std::mutex> g(c.mu);
   while (fgets(line, sizeof line, f)) {
-    int a[12];
+    int a[13];
     if (line[0] == '#' || line[0] == '\n') continue;
     if (sscanf(line, "choice %d %d %d %d %d %d %d %d %d %d %d %d", &a[0], &a[1], &a[2],
                &a[3], &a[4], &a[5], &a[6], &a[7], &a[8], &a[9], &a[10], &a[11]) == 12) {
       if (a[9] < 1 || a[10] < 1 || a[10] > 8 || a[11] < 1) { ++bad; continue; }
       c.choices[TuneKey{a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8]}] =
           TuneChoice{a[9], a[10], a[11]};
-    } else if (sscanf(line, "choice3d %d %d %d %d %d %d %d %d %d %d %d", &a[0], &a[1], &a[2],
-                      &a[3], &a[4], &a[5], &a[6], &a[7], &a[8], &a[9], &a[10]) == 11) {
-      if (a[7] < 1 || a[8] < 1 || a[9] < 1 || a[10] < 0 || a[10] > 1) { ++bad; continue; }
+    } else if (sscanf(line, "choice3d %d %d %d %d %d %d %d %d %d %d %d %d", &a[0], &a[1],
+                      &a[2], &a[3], &a[4], &a[5], &a[6], &a[7], &a[8], &a[9], &a[10],
+                      &a[11]) == 12) {
+      if (a[7] < 1 || a[8] < 1 || a[9] < 1 || a[10] < 0 || a[10] > 1 || a[11] < 1) {
+        ++bad;
+        continue;
+      }
       tune3d_store(a, a + 7);
     } else if (sscanf(line, "depth %d %d %d %d %d %d %d %d %d", &a[0], &a[1], &a[2], &a[3],
                       &a[4], &a[5], &a[6], &a[7], &a[8]) == 9) {

@@ -23,9 +23,9 @@ int tune_depth_2d(int dtype, int rl, int rr, int rt, int rb, int star, int64_t w
                   int64_t h, int steps);
 
 // The 3D autotuner's measured choices (stencil3d.cu): key = (dtype, shape,
-// radius, rhs, log2 nx, log2 ny, log2 nz*nbatch), value = (PY, NW, S, zreg).
-void tune3d_for_each(void (*cb)(const int key[7], const int val[4], void*), void* user);
-void tune3d_store(const int key[7], const int val[4]);
+// radius, rhs, log2 nx, log2 ny, log2 nz*nbatch), value = (PY, NW, S, zreg, V).
+void tune3d_for_each(void (*cb)(const int key[7], const int val[5], void*), void* user);
+void tune3d_store(const int key[7], const int val[5]);
 void tune3d_clear();
 
 }  // namespace ssam

@@ -73,9 +73,9 @@ static const std::vector<Cand3D>* cands_3d(int dtype, int shape, int r, bool rhs
 }
 
 // Measured choices: (dtype, shape, radius, rhs, log2 nx, log2 ny, log2 nz*nb)
-// -> (PY, NW, S, zreg).
+// -> (PY, NW, S, zreg, V).
 using Tune3DKey = std::tuple<int, int, int, int, int, int, int>;
-using Tune3DVal = std::tuple<int, int, int, int>;
+using Tune3DVal = std::tuple<int, int, int, int, int>;
 static std::mutex g_tune3_mu;
 static std::map<Tune3DKey, Tune3DVal> g_tune3;
 
@@ -105,29 +105,29 @@ static const Cand3D* pick_3d(int dtype, int shape, int r, bool rhs, int64_t nx, 
     auto it = g_tune3.find(tune3_key(dtype, shape, r, rhs, nx, ny, nzb));
     if (it != g_tune3.end())
       for (const Cand3D& c : *cs)
-        if (Tune3DVal{c.py, c.nw, c.s, c.zreg} == it->second) return &c;
+        if (Tune3DVal{c.py, c.nw, c.s, c.zreg, c.v} == it->second) return &c;
   }
   for (const Cand3D& c : *cs)
     if (c.dflt) return &c;
   return &cs->front();
 }
 
-void tune3d_for_each(void (*cb)(const int key[7], const int val[4], void*), void* user) {
+void tune3d_for_each(void (*cb)(const int key[7], const int val[5], void*), void* user) {
   std::lock_guard<std::mutex> g(g_tune3_mu);
   for (auto& kv : g_tune3) {
     const int k[7] = {std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first),
                       std::get<3>(kv.first), std::get<4>(kv.first), std::get<5>(kv.first),
                       std::get<6>(kv.first)};
-    const int v[4] = {std::get<0>(kv.second), std::get<1>(kv.second), std::get<2>(kv.second),
-                      std::get<3>(kv.second)};
+    const int v[5] = {std::get<0>(kv.second), std::get<1>(kv.second), std::get<2>(kv.second),
+                      std::get<3>(kv.second), std::get<4>(kv.second)};
     cb(k, v, user);
   }
 }
 
-void tune3d_store(const int key[7], const int val[4]) {
+void tune3d_store(const int key[7], const int val[5]) {
   std::lock_guard<std::mutex> g(g_tune3_mu);
   g_tune3[Tune3DKey{key[0], key[1], key[2], key[3], key[4], key[5], key[6]}] =
-      Tune3DVal{val[0], val[1], val[2], val[3]};
+      Tune3DVal{val[0], val[1], val[2], val[3], val[4]};
 }
 
 void tune3d_clear() {
@@ -378,13 +378,14 @@ static int tune_3d(const std::vector<Cand3D>& cs, const Launch3D& a, const Tune3
                                      std::to_string(code) + ")");
   {
     std::lock_guard<std::mutex> g(g_tune3_mu);
-    g_tune3[key] = Tune3DVal{best->py, best->nw, best->s, best->zreg};
+    g_tune3[key] = Tune3DVal{best->py, best->nw, best->s, best->zreg, best->v};
   }
   if (report) {
     report->rows_per_warp = best->py;
     report->consumer_warps = best->nw;
     report->ring_slots = best->s;
     report->registers_z = best->zreg;
+    report->columns_per_thread = best->v;
     report->candidates = timed;
     report->ms_per_step = best_ms;
   }

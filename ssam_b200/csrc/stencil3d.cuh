@@ -3,12 +3,15 @@
 // Method (the reference's 3D scheme, ssai-3dstencil/tmp3d7pt-v2.cu:62-208:
 // "y-strip in registers, x by shuffles, z through shared memory"), laid out
 // for Blackwell:
-//   * a CTA owns column tiles of 128 x TY cells and walks them along z.  A
-//     producer warp stages each z-plane of the tile -- 128 + 2*HX columns by
+//   * a CTA owns column tiles of 32*V x TY cells and walks them along z.  A
+//     producer warp stages each z-plane of the tile -- 32*V + 2*HX columns by
 //     TY + 2*RY rows, halos included -- into a ring of S shared-memory slots
-//     with one cp.async.bulk.tensor (TMA, no multicast) per plane, signalled
-//     through mbarriers (full: bytes landed; empty: consumers are done);
-//   * NW consumer warps each own a 128 x PY strip.  A thread owns V = 4
+//     with one cp.async.bulk.tensor (TMA, no multicast) per plane, or two
+//     when the row is wider than a TMA box (256 elements; V = 8: the left
+//     half with the left halo, the right half with the right one, stored one
+//     after the other in the slot), signalled through mbarriers (full: bytes
+//     landed; empty: consumers are done);
+//   * NW consumer warps each own a 32*V x PY strip.  A thread owns V (4 or 8)
 //     consecutive columns; for every plane of the stencil it reads its rows
 //     (plus the y reach) from the slot into registers, forms its own
 //     contributions and the partial sums destined for the neighbouring
@@ -65,23 +68,44 @@ __host__ __device__ constexpr int rx3(int dz, int dy) {
   return m;
 }
 
-template <typename TS, int SH, int R, int PY, int NW, int S>
+// V columns a thread (4, or 8: a 256-column tile).  A plane of the tile with
+// its halo columns is staged as NBOX boxes side by side (one TMA copy each:
+// a box is at most 256 elements wide), box b holding columns b*BW .. of the
+// staged row; a lane reads only its own box (lanes 0..15 the first, 16..31 the
+// second when NBOX = 2, and the halo columns lanes 0 / 31 need are in theirs).
+template <typename TS, int SH, int R, int PY, int NW, int S, int V_ = 4>
 struct Stencil3DCfg {
   using TA = typename Traits<TS>::TA;
-  static constexpr int V = 4;                       // columns per thread
-  static constexpr int TX = 128;                    // tile columns
+  static constexpr int V = V_;                      // columns per thread
+  static constexpr int TX = 32 * V;                 // tile columns
   static constexpr int HX = 16 / (int)sizeof(TS);   // halo columns (16 bytes)
   static constexpr int TY = NW * PY;                // tile rows
   static constexpr int RYM = ry3<SH, R>(0) > 0 ? ry3<SH, R>(0) : 1;  // max y reach
-  static constexpr int XW = TX + 2 * HX;            // slot row length
+  static constexpr int NBOX = TX + 2 * HX > 256 ? 2 : 1;  // staged boxes per plane
+  static constexpr int BW = (TX + 2 * HX) / NBOX;   // box width (elements)
+  static constexpr int XW = BW;                     // slot row length (within a box)
   static constexpr int YW = TY + 2 * RYM;           // slot rows
-  static constexpr int SLOT_BYTES = ((XW * YW * (int)sizeof(TS)) + 127) / 128 * 128;
+  static constexpr int BOXE = BW * YW;              // elements of one box
+  // element stride between the boxes of a slot: a TMA copy's shared-memory
+  // destination must be 128-byte aligned
+  static constexpr int BOXS = (BOXE * (int)sizeof(TS) + 127) / 128 * 128 / (int)sizeof(TS);
+  static constexpr int LPB = 32 / NBOX;             // lanes reading one box
+  static constexpr int SLOT_BYTES = NBOX * BOXS * (int)sizeof(TS);
+  // element offset, within a slot, of row 0 / a lane's first column
+  __host__ __device__ static constexpr int col_off(int lane) {
+    return (lane / LPB) * BOXS + (lane / LPB == 0 ? HX : 0) + (lane % LPB) * V;
+  }
+  static_assert(NBOX == 1 || (TX / 2 + HX) * (int)sizeof(TS) % 16 == 0,
+                "the second box must start on a 16-byte column");
+  static_assert((BOXS * (int)sizeof(TS)) % 128 == 0 && SLOT_BYTES % 128 == 0,
+                "every box of every slot starts on a 128-byte boundary");
   static constexpr int SMEM = S * SLOT_BYTES + 2 * S * 8 + 128;
   static constexpr int NC = (2 * R + 1) * (2 * R + 1) * (2 * R + 1);
   static constexpr int THREADS = 32 * (NW + 1);
   // CTAs per SM the register budget is cut for: two when two rings fit in
-  // shared memory and the CTA is at most 9 warps, else one
-  static constexpr int MINB = (NW < 12 && 2 * (SMEM + 1024) <= 233472) ? 2 : 1;
+  // shared memory and the CTA is at most 12 warps of 4-column threads, else
+  // one (8-column threads hold twice the cells and would spill at half)
+  static constexpr int MINB = (V == 4 && NW < 12 && 2 * (SMEM + 1024) <= 233472) ? 2 : 1;
   static_assert(R <= HX && R <= V, "x reach must fit in the halo and one lane hop");
 };
 
@@ -247,18 +271,22 @@ __device__ __forceinline__ void produce_planes(const CUtensorMap& map, const TS*
       TS* slot = slots + (size_t)s * (C::SLOT_BYTES / sizeof(TS));
       if (w.use_tma) {
         if (lane == 0) {
-          mbar_expect_tx(&full[s], (unsigned)(XW * C::YW * sizeof(TS)));
-          tma_load_plane(slot, &map, gx, gy, (int)p, (int)sg.b, &full[s]);
+          mbar_expect_tx(&full[s], (unsigned)(C::NBOX * C::BOXE * sizeof(TS)));
+#pragma unroll
+          for (int b = 0; b < C::NBOX; ++b)
+            tma_load_plane(slot + b * C::BOXS, &map, gx + b * XW, gy, (int)p, (int)sg.b,
+                           &full[s]);
         }
       } else {
         // plain loads for grids whose rows are not 16-byte multiples
-        for (int i = lane; i < XW * C::YW; i += 32) {
-          const int r = i / XW, c = i % XW;
-          const int64_t x = gx + c, y = gy + r;
+        for (int i = lane; i < C::NBOX * C::BOXE; i += 32) {
+          const int b = i / C::BOXE, e = i % C::BOXE;
+          const int r = e / XW, c = e % XW;
+          const int64_t x = gx + b * XW + c, y = gy + r;
           TS v = from_acc<TS>(TA(0));
           if (x >= 0 && x < nx && y >= 0 && y < ny && p >= 0 && p < nz)
             v = src[(sg.b * nz + p) * nxy + y * nx + x];
-          slot[r * XW + c] = v;
+          slot[b * C::BOXS + e] = v;
         }
         mbar_arrive(&full[s]);
       }
@@ -276,13 +304,13 @@ __device__ __forceinline__ void produce_planes(const CUtensorMap& map, const TS*
 // RHS: the Jacobi form out = stencil(in) + rhs_scale * rhs.  Its rows are
 // loaded at the top of every plane, so their latency overlaps the plane's
 // barrier waits and arithmetic (instances without it carry no rhs code).
-template <typename TS, int SH, int R, int PY, int NW, int S, bool RHS = false>
-__global__ void __launch_bounds__(32 * (NW + 1), (Stencil3DCfg<TS, SH, R, PY, NW, S>::MINB))
+template <typename TS, int SH, int R, int PY, int NW, int S, bool RHS = false, int V_ = 4>
+__global__ void __launch_bounds__(32 * (NW + 1), (Stencil3DCfg<TS, SH, R, PY, NW, S, V_>::MINB))
 stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__ src,
                  TS* __restrict__ dst, Work3D w,
                  CoefBlock<typename Traits<TS>::TA,
-                           Stencil3DCfg<TS, SH, R, PY, NW, S>::NC> cf) {
-  using C = Stencil3DCfg<TS, SH, R, PY, NW, S>;
+                           Stencil3DCfg<TS, SH, R, PY, NW, S, V_>::NC> cf) {
+  using C = Stencil3DCfg<TS, SH, R, PY, NW, S, V_>;
   using TA = typename C::TA;
   constexpr int V = C::V, XW = C::XW, HX = C::HX, RYM = C::RYM, TY = C::TY;
   constexpr int F = 2 * R + 1;
@@ -320,7 +348,7 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
     const int tx = (int)(sg.tile % w.ntx), ty = (int)(sg.tile / w.ntx);
     const int64_t x0 = (int64_t)tx * C::TX + lane * V;  // my first column
     const int64_t y0 = (int64_t)ty * TY + warp * PY;    // my first row
-    const int col = HX + lane * V;                      // my first column in a slot
+    const int col = C::col_off(lane);                   // my first column in a slot
     const int row0 = RYM + warp * PY;                   // my first row in a slot
     const int64_t seg_planes = sg.zb - sg.za + 2 * R;
     // does my strip touch the x/y ring that COPY keeps?

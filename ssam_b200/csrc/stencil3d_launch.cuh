@@ -47,13 +47,13 @@ struct Launch3D {
 // ZREG: the kernel of stencil3d_zreg.cuh (own cells in a register ring
 // along z) instead of stencil3d_kernel.
 template <typename TS, int SH, int R, int PY, int NW, int S, bool RHS = false,
-          bool ZREG = false>
+          bool ZREG = false, int V_ = 4>
 int launch_3d(const Launch3D& a) {
-  using C = Stencil3DCfg<TS, SH, R, PY, NW, S>;
+  using C = Stencil3DCfg<TS, SH, R, PY, NW, S, V_>;
   using TA = typename C::TA;
   auto kern = [] {
-    if constexpr (ZREG) return &stencil3d_zreg_kernel<TS, SH, R, PY, NW, S, RHS>;
-    else return &stencil3d_kernel<TS, SH, R, PY, NW, S, RHS>;
+    if constexpr (ZREG) return &stencil3d_zreg_kernel<TS, SH, R, PY, NW, S, RHS, V_>;
+    else return &stencil3d_kernel<TS, SH, R, PY, NW, S, RHS, V_>;
   }();
   if ((a.rhs != nullptr) != RHS)
     return fail(SSAM_ERR_INVALID, "3D kernel instance does not match the right-hand side");
@@ -119,7 +119,7 @@ int launch_3d(const Launch3D& a) {
                           (cuuint64_t)a.nb};
     cuuint64_t strides[3] = {(cuuint64_t)(a.nx * es), (cuuint64_t)(a.nx * a.ny * es),
                              (cuuint64_t)(a.nx * a.ny * a.nz * es)};
-    cuuint32_t box[4] = {(cuuint32_t)C::XW, (cuuint32_t)C::YW, 1, 1};
+    cuuint32_t box[4] = {(cuuint32_t)C::BW, (cuuint32_t)C::YW, 1, 1};
     cuuint32_t estr[4] = {1, 1, 1, 1};
     CUresult r = tensor_map_encoder()(&map, tma_dtype<TS>(), 4, const_cast<void*>(a.src), dims,
                              strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -141,13 +141,15 @@ int launch_3d(const Launch3D& a) {
 using LaunchFn3D = int (*)(const Launch3D&);
 
 // One compiled configuration of a 3D stencil: rows per consumer warp (PY),
-// consumer warps per CTA (NW; the column tile is 128 x NW*PY), ring slots
-// (S planes of the tile in shared memory) and the kernel variant.  `dflt` marks the configuration
+// consumer warps per CTA (NW; the column tile is 32*V x NW*PY), ring slots
+// (S planes of the tile in shared memory), the kernel variant and the
+// columns a thread (V).  `dflt` marks the configuration
 // used when nothing was measured for the grid's size class.
 struct Cand3D {
   LaunchFn3D fn;
   int py, nw, s;
   int zreg;  // 1: own cells in a register ring along z (stencil3d_zreg.cuh)
+  int v;     // columns a thread (the tile is 32*v columns)
   bool dflt;
 };
 
@@ -155,12 +157,12 @@ struct Cand3D {
 void register_3d(int dtype, int shape, int r, bool rhs, const Cand3D& c);
 
 template <typename TS, int SH, int R, int PY, int NW, int S, bool RHS, bool DEFAULT,
-          bool ZREG = false>
+          bool ZREG = false, int V_ = 4>
 struct Register3D {
   Register3D() {
     register_3d(Traits<TS>::DT, SH, R, RHS,
-                Cand3D{&launch_3d<TS, SH, R, PY, NW, S, RHS, ZREG>, PY, NW, S, ZREG ? 1 : 0,
-                       DEFAULT});
+                Cand3D{&launch_3d<TS, SH, R, PY, NW, S, RHS, ZREG, V_>, PY, NW, S, ZREG ? 1 : 0,
+                       V_, DEFAULT});
   }
 };
 

@@ -36,13 +36,13 @@ __host__ __device__ constexpr int halo_reach_z() {
   return m;
 }
 
-template <typename TS, int SH, int R, int PY, int NW, int S, bool RHS = false>
-__global__ void __launch_bounds__(32 * (NW + 1), (Stencil3DCfg<TS, SH, R, PY, NW, S>::MINB))
+template <typename TS, int SH, int R, int PY, int NW, int S, bool RHS = false, int V_ = 4>
+__global__ void __launch_bounds__(32 * (NW + 1), (Stencil3DCfg<TS, SH, R, PY, NW, S, V_>::MINB))
 stencil3d_zreg_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__ src,
                       TS* __restrict__ dst, Work3D w,
                       CoefBlock<typename Traits<TS>::TA,
-                                Stencil3DCfg<TS, SH, R, PY, NW, S>::NC> cf) {
-  using C = Stencil3DCfg<TS, SH, R, PY, NW, S>;
+                                Stencil3DCfg<TS, SH, R, PY, NW, S, V_>::NC> cf) {
+  using C = Stencil3DCfg<TS, SH, R, PY, NW, S, V_>;
   using TA = typename C::TA;
   constexpr int V = C::V, XW = C::XW, HX = C::HX, RYM = C::RYM, TY = C::TY;
   constexpr int F = 2 * R + 1;
@@ -82,7 +82,7 @@ stencil3d_zreg_kernel(const __grid_constant__ CUtensorMap map, const TS* __restr
     const int tx = (int)(sg.tile % w.ntx), ty = (int)(sg.tile / w.ntx);
     const int64_t x0 = (int64_t)tx * C::TX + lane * V;  // my first column
     const int64_t y0 = (int64_t)ty * TY + warp * PY;    // my first row
-    const int col = HX + lane * V;                      // my first column in a slot
+    const int col = C::col_off(lane);                   // my first column in a slot
     const int row0 = RYM + warp * PY;                   // my first row in a slot
     const int nzc = (int)(sg.zb - sg.za);
     // does my strip touch the x/y ring that COPY keeps?

@@ -98,23 +98,24 @@ def test_autotune_cache_file_roundtrip(tmp_path):
 
 def test_autotune_3d_choices_roundtrip(tmp_path):
     """The 3D autotuner's choices (choice3d lines: dtype, shape, radius, rhs,
-    size class, PY, NW, S, z-register flag) persist beside the 2D ones; bad
+    size class, PY, NW, S, z-register flag, V) persist beside the 2D ones; bad
     lines are rejected; clearing forgets both kinds (no GPU)."""
     S.autotune_clear()
     p = tmp_path / "tune3d.txt"
     p.write_text("# ssam_b200 autotune cache v1\n"
                  "choice 0 2 2 2 2 0 1 13 13 32 2 4\n"
-                 "choice3d 0 0 2 0 9 9 9 2 16 8 1\n"
-                 "choice3d 2 0 1 1 7 7 10 4 8 6 0\n")
+                 "choice3d 0 0 2 0 9 9 9 2 16 8 1 4\n"
+                 "choice3d 2 0 1 1 7 7 10 4 8 6 0 8\n")
     S.autotune_load(str(p))
     q = tmp_path / "again.txt"
     S.autotune_save(str(q))
     text = q.read_text()
-    assert "choice3d 0 0 2 0 9 9 9 2 16 8 1" in text
-    assert "choice3d 2 0 1 1 7 7 10 4 8 6 0" in text
+    assert "choice3d 0 0 2 0 9 9 9 2 16 8 1 4" in text
+    assert "choice3d 2 0 1 1 7 7 10 4 8 6 0 8" in text
     assert "choice 0 2 2 2 2 0 1 13 13 32 2 4" in text
-    for bad_line in ("choice3d 0 0 2 0 9 9 9 2 16 8 2\n",   # z flag must be 0 or 1
-                     "choice3d 0 0 2 0 9 9 9 0 16 8 1\n",   # PY >= 1
+    for bad_line in ("choice3d 0 0 2 0 9 9 9 2 16 8 2 4\n",   # z flag must be 0 or 1
+                     "choice3d 0 0 2 0 9 9 9 0 16 8 1 4\n",   # PY >= 1
+                     "choice3d 0 0 2 0 9 9 9 2 16 8 1 0\n",   # V >= 1
                      "choice3d 0 0 2 0 9 9\n"):
         bad = tmp_path / "bad3d.txt"
         bad.write_text(bad_line)

@@ -12,23 +12,28 @@ ES = {"f32": 4, "f64": 8, "bf16": 2, "f16": 2}
 SMEM_PER_CTA = 227 * 1024
 
 
-def smem_3d(dt, shape, r, py, nw, s):
+def smem_3d(dt, shape, r, py, nw, s, v=4):
     """Dynamic shared memory of a 3D CTA as the launcher requests it
-    (Stencil3DCfg::SMEM): S slots of (128 + 2*HX) x (NW*PY + 2*RYM) elements
-    rounded to 128 bytes, two mbarriers per slot, 128 bytes of alignment."""
+    (Stencil3DCfg::SMEM): S slots of (32*V + 2*HX) x (NW*PY + 2*RYM) elements,
+    staged as one box (or two halves when wider than 256 elements), each box
+    rounded to 128 bytes; two mbarriers per slot, 128 bytes of alignment."""
     es = ES[dt]
     hx = 16 // es
-    xw = 128 + 2 * hx
+    xw = 32 * v + 2 * hx
+    nbox = 2 if xw > 256 else 1
     rym = 1 if shape == 1 else r
     yw = nw * py + 2 * rym
-    slot = (xw * yw * es + 127) // 128 * 128
+    slot = nbox * ((xw // nbox * yw * es + 127) // 128 * 128)
     return s * slot + 2 * s * 8 + 128
 
 
 @pytest.mark.parametrize("inst", instances_3d(), ids=lambda c: "-".join(map(str, c)))
 def test_3d_configuration_fits_and_has_its_ring(inst):
-    dt, shape, r, py, nw, s, rhs, dflt, zreg = inst
-    assert smem_3d(dt, shape, r, py, nw, s) <= SMEM_PER_CTA
+    dt, shape, r, py, nw, s, rhs, dflt, zreg, v = inst
+    assert smem_3d(dt, shape, r, py, nw, s, v) <= SMEM_PER_CTA
+    if v == 8:  # two TMA boxes of at most 256 elements, 16-byte rows
+        bw = (32 * v + 2 * (16 // ES[dt])) // 2
+        assert bw <= 256 and (bw * ES[dt]) % 16 == 0
     assert 32 * (nw + 1) <= 1024
     rh = 1 if shape == 1 else 0  # planes read for halos: z-RH .. z+RH
     need = r + rh + 2 if zreg else 2 * r + 2
@@ -38,14 +43,14 @@ def test_3d_configuration_fits_and_has_its_ring(inst):
 
 
 def test_3d_groups_have_exactly_one_default():
-    groups = Counter((dt, shape, r, rhs) for (dt, shape, r, _, _, _, rhs, dflt, _)
+    groups = Counter((dt, shape, r, rhs) for (dt, shape, r, _, _, _, rhs, dflt, _, _)
                      in instances_3d() if dflt)
-    every = {(dt, shape, r, rhs) for (dt, shape, r, _, _, _, rhs, _, _) in instances_3d()}
+    every = {(dt, shape, r, rhs) for (dt, shape, r, _, _, _, rhs, _, _, _) in instances_3d()}
     assert set(groups) == every and all(v == 1 for v in groups.values())
 
 
 def test_3d_table_covers_the_entry_points():
-    have = {(dt, shape, r, rhs) for (dt, shape, r, _, _, _, rhs, _, _) in instances_3d()}
+    have = {(dt, shape, r, rhs) for (dt, shape, r, _, _, _, rhs, _, _, _) in instances_3d()}
     for dt in ("f32", "f64", "bf16", "f16"):
         for shape, r in ((0, 1), (0, 2), (1, 1)):
             assert (dt, shape, r, False) in have

@@ -1,6 +1,7 @@
 """Every compiled 3D configuration (rows per warp PY, consumer warps NW,
-ring slots S, and the variant with each thread's own cells in a register
-ring along z) against the oracle, and the 3D autotuners.
+ring slots S, the variant with each thread's own cells in a register ring
+along z, and columns a thread V: 4, or 8 with each plane staged as two TMA
+boxes) against the oracle, and the 3D autotuners.
 
 A configuration is pinned for the grid's size class through a tune-cache
 file (``choice3d`` lines, read by ssam_autotune_load), the public way to fix
@@ -31,20 +32,20 @@ def log2(v):
 
 
 def pin(tmp_path, dt, shape, r, rhs, nx, ny, nzb, cfg):
-    py, nw, s, zreg = cfg
+    py, nw, s, zreg, v = cfg
     p = tmp_path / "pin3d.txt"
     p.write_text("# ssam_b200 autotune cache v1\n"
                  f"choice3d {DTC[dt]} {shape} {r} {int(rhs)} {log2(nx)} {log2(ny)} {log2(nzb)} "
-                 f"{py} {nw} {s} {int(zreg)}\n")
+                 f"{py} {nw} {s} {int(zreg)} {v}\n")
     S.autotune_clear()
     S.autotune_load(str(p))
 
 
 def stencil_cases():
     out = []
-    for (dt, shape, r, py, nw, s, rhs, _, zreg) in instances_3d():
+    for (dt, shape, r, py, nw, s, rhs, _, zreg, v) in instances_3d():
         if not rhs and dt in ("f32", "f64", "bf16"):
-            out.append((dt, shape, r, (py, nw, s, zreg)))
+            out.append((dt, shape, r, (py, nw, s, zreg, v)))
     return out
 
 
@@ -56,12 +57,13 @@ def cube_for(shape, r):
 
 
 def case_id(c):
-    dt, shape, r, (py, nw, s, zreg) = c
-    return f"{dt}-{'p19' if shape else 'star'}{r}-{py}x{nw}x{s}{'z' if zreg else ''}"
+    dt, shape, r, (py, nw, s, zreg, v) = c
+    return (f"{dt}-{'p19' if shape else 'star'}{r}-{py}x{nw}x{s}{'z' if zreg else ''}"
+            f"{'-v8' if v == 8 else ''}")
 
 
 @pytest.mark.parametrize("dt,shape,r,cfg", stencil_cases(), ids=[case_id(c) for c in stencil_cases()])
-@pytest.mark.parametrize("dims", [(40, 75, 200), (19, 33, 130)])
+@pytest.mark.parametrize("dims", [(40, 75, 296), (19, 33, 130)])
 @pytest.mark.parametrize("bnd", ["zero", "copy"])
 def test_every_3d_configuration_vs_oracle(cuda, tmp_path, dt, shape, r, cfg, dims, bnd):
     nz, ny, nx = dims
@@ -87,13 +89,13 @@ def test_every_3d_configuration_vs_oracle(cuda, tmp_path, dt, shape, r, cfg, dim
 
 
 def sweep_cases():
-    return [(dt, (py, nw, s, zreg)) for (dt, shape, r, py, nw, s, rhs, _, zreg) in instances_3d()
-            if rhs]
+    return [(dt, (py, nw, s, zreg, v))
+            for (dt, shape, r, py, nw, s, rhs, _, zreg, v) in instances_3d() if rhs]
 
 
 @pytest.mark.parametrize("dt,cfg", sweep_cases(),
                          ids=[f"{d}-{c[0]}x{c[1]}x{c[2]}{'z' if c[3] else ''}"
-                              for d, c in sweep_cases()])
+                              f"{'-v8' if c[4] == 8 else ''}" for d, c in sweep_cases()])
 def test_every_jacobi_configuration_vs_oracle(cuda, tmp_path, dt, cfg):
     n, nb, sweeps = 24, 3, 2
     rel = {"f64": 1e-12, "f32": 1e-5, "bf16": 2.0**-8}[dt]
