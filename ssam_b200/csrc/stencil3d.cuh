@@ -458,12 +458,15 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
           if (k < -ry || k >= PY + ry) continue;
           const TS* rowp = slot + (row0 + k) * XW + col;
           load_slot_row<TS, V>(d[k + ry], rowp);
-          // every lane reads the columns beyond its strip on the side that
-          // matters to lane 0 / lane 31; only those two lanes use the result
-          // (no divergent branch: the warp issues the load once either way)
+          // the x-halo columns, used by lanes 0 and 31 only: lane 0 reads
+          // left of its strip and every other lane reads lane 31's right halo
+          // column, so the warp touches two addresses (a broadcast, no bank
+          // conflict) and issues the load once
+          const TS* hrow = slot + (row0 + k) * XW;
 #pragma unroll
           for (int h = 0; h < R; ++h)
-            hv[k + ry][h] = to_acc(rowp[lane == 0 ? -1 - h : V + h]);
+            hv[k + ry][h] =
+                to_acc(hrow[lane == 0 ? C::col_off(0) - 1 - h : C::col_off(31) + V + h]);
         }
         if (dz == 0) {
 #pragma unroll

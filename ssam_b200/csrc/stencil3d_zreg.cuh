@@ -225,10 +225,14 @@ stencil3d_zreg_kernel(const __grid_constant__ CUtensorMap map, const TS* __restr
               load_slot_row<TS, V>(d[k + ry], rowp);
             }
             // x halo for lanes 0 / 31 (the loads whose values no tap uses are
-            // dropped by the compiler)
+            // dropped by the compiler): lane 0 reads left of its strip, every
+            // other lane lane 31's right halo column -- two addresses a warp,
+            // a broadcast without bank conflicts
+            const TS* hrow = sl + (row0 + k) * XW;
 #pragma unroll
             for (int h = 0; h < R; ++h)
-              hv[k + ry][h] = to_acc(rowp[lane == 0 ? -1 - h : V + h]);
+              hv[k + ry][h] =
+                  to_acc(hrow[lane == 0 ? C::col_off(0) - 1 - h : C::col_off(31) + V + h]);
           }
 #pragma unroll
           for (int i = 0; i < PY; ++i) {
