@@ -291,7 +291,7 @@ static int poisson_solve(const double* f, double* u, int n, int nbatch,
   std::vector<double> norms2(2 * nbatch);
   bool use_cnn = cnn != nullptr;
   bool first = true;
-  bool judge_cnn = false;  // the last cycle used the network
+  bool cnn_on_trial = false;  // the last cycle used the network
   double before_cnn = 0.0;
 
   ssam_poisson_stats local = {};
@@ -327,8 +327,8 @@ static int poisson_solve(const double* f, double* u, int n, int nbatch,
         continue;
       }
     }
-    if (judge_cnn) {
-      judge_cnn = false;
+    if (cnn_on_trial) {
+      cnn_on_trial = false;
       if (worst < 0.9 * before_cnn) {
         out->cnn_corrections += 1;
       } else {
@@ -361,7 +361,7 @@ static int poisson_solve(const double* f, double* u, int n, int nbatch,
         break;
       }
       before_cnn = worst;
-      judge_cnn = true;
+      cnn_on_trial = true;
       // the network sees the smooth part of r, and its BF16 noise is
       // filtered out of the correction (the sweeps handle the rest)
       const double* cin = r64;

@@ -1,6 +1,6 @@
 """The Poisson path: Jacobi sweeps (the 3D TMA stencil kernel with a
 right-hand side) and the FP64 residual against the FP64 oracle, and the
-defect-correction solve reaching its tolerance as judged by the oracle."""
+defect-correction solve reaching its tolerance as checked by the oracle."""
 import numpy as np
 import pytest
 import torch

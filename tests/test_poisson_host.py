@@ -1,6 +1,6 @@
 """Host-side pieces of the learned Poisson arm: the device RHS generator
 matches the numpy one, and the sine-transform solve that makes the training
-targets gives the exact discrete solution (judged by the FP64 oracle)."""
+targets gives the exact discrete solution (checked by the FP64 oracle)."""
 import numpy as np
 import pytest
 import torch
