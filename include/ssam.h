@@ -297,7 +297,16 @@ SSAM_API int ssam_autotune_jacobi3d(int64_t n, int nbatch, int sweep_dtype, void
                                     ssam_tune3d_report* report);
 
 /* Persist / restore / forget the measured choices of the 2D and 3D
- * autotuners (a small text file). */
+ * autotuners.  The file is text, one choice a line ('#' starts a comment):
+ *   choice   dtype rl rr rt rb star t log2w log2h P warps V
+ *   depth    dtype rl rr rt rb star log2w log2h t
+ *   choice3d dtype shape radius rhs log2nx log2ny log2(nz*nbatch) PY NW S zreg V
+ * (t: time steps fused in one launch; P: rows a thread, or the streaming
+ * segment; V: columns a thread)
+ * (a choice3d line without its last field means V = 4).  Writing such lines
+ * by hand pins a configuration; load fails with SSAM_ERR_INVALID, naming the
+ * count of malformed lines, when a line does not parse or a value is out of
+ * range, after loading the good ones. */
 SSAM_API int ssam_autotune_save(const char* path);
 SSAM_API int ssam_autotune_load(const char* path);
 SSAM_API int ssam_autotune_clear(void);

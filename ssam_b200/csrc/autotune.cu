@@ -293,9 +293,11 @@ extern "C" int ssam_autotune_load(const char* path) {
       if (a[9] < 1 || a[10] < 1 || a[10] > 8 || a[11] < 1) { ++bad; continue; }
       c.choices[TuneKey{a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8]}] =
           TuneChoice{a[9], a[10], a[11]};
-    } else if (sscanf(line, "choice3d %d %d %d %d %d %d %d %d %d %d %d %d", &a[0], &a[1],
-                      &a[2], &a[3], &a[4], &a[5], &a[6], &a[7], &a[8], &a[9], &a[10],
-                      &a[11]) == 12) {
+    } else if (int n3 = sscanf(line, "choice3d %d %d %d %d %d %d %d %d %d %d %d %d", &a[0],
+                               &a[1], &a[2], &a[3], &a[4], &a[5], &a[6], &a[7], &a[8], &a[9],
+                               &a[10], &a[11]);
+               n3 == 11 || n3 == 12) {
+      if (n3 == 11) a[11] = 4;  // lines written before the V field: 4 columns a thread
       if (a[7] < 1 || a[8] < 1 || a[9] < 1 || a[10] < 0 || a[10] > 1 || a[11] < 1) {
         ++bad;
         continue;

@@ -121,6 +121,12 @@ def test_autotune_3d_choices_roundtrip(tmp_path):
         bad.write_text(bad_line)
         with pytest.raises(S.SsamError):
             S.autotune_load(str(bad))
+    # a line saved before the columns-a-thread field reads as V = 4
+    old = tmp_path / "old3d.txt"
+    old.write_text("choice3d 1 1 1 0 8 8 8 4 4 5 0\n")
+    S.autotune_load(str(old))
+    S.autotune_save(str(q))
+    assert "choice3d 1 1 1 0 8 8 8 4 4 5 0 4" in q.read_text()
     S.autotune_clear()
     S.autotune_save(str(q))
     assert "choice3d" not in q.read_text()
