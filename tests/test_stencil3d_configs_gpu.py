@@ -62,10 +62,7 @@ def case_id(c):
             f"{'-v8' if v == 8 else ''}")
 
 
-@pytest.mark.parametrize("dt,shape,r,cfg", stencil_cases(), ids=[case_id(c) for c in stencil_cases()])
-@pytest.mark.parametrize("dims", [(40, 75, 296), (19, 33, 130)])
-@pytest.mark.parametrize("bnd", ["zero", "copy"])
-def test_every_3d_configuration_vs_oracle(cuda, tmp_path, dt, shape, r, cfg, dims, bnd):
+def check_configuration(cuda, tmp_path, dt, shape, r, cfg, dims, bnd):
     nz, ny, nx = dims
     cube, sh = cube_for(shape, r)
     src32 = uniform(dims, -1, 1, np.float32, nx + 7 * r + shape)
@@ -86,6 +83,29 @@ def test_every_3d_configuration_vs_oracle(cuda, tmp_path, dt, shape, r, cfg, dim
         want = oracle_steps(src, cube.astype(src.dtype), 1, bnd)
         rel = 1e-5 if dt == "f32" else 1e-12
         band_close(got, want, magnitude(src, cube, 1, bnd), 0, rel, f"{dt} {cfg}")
+
+
+@pytest.mark.parametrize("dt,shape,r,cfg", stencil_cases(), ids=[case_id(c) for c in stencil_cases()])
+@pytest.mark.parametrize("dims", [(40, 75, 296), (19, 33, 130)])
+@pytest.mark.parametrize("bnd", ["zero", "copy"])
+def test_every_3d_configuration_vs_oracle(cuda, tmp_path, dt, shape, r, cfg, dims, bnd):
+    check_configuration(cuda, tmp_path, dt, shape, r, cfg, dims, bnd)
+
+
+def wide_cases():
+    return [c for c in stencil_cases() if c[3][4] == 8]
+
+
+@pytest.mark.parametrize("dt,shape,r,cfg", wide_cases(), ids=[case_id(c) for c in wide_cases()])
+@pytest.mark.parametrize("dims", [(6, 10, 44), (5, 7, 136)])
+@pytest.mark.parametrize("bnd", ["zero", "copy"])
+def test_8_column_tiles_on_narrow_grids(cuda, tmp_path, dt, shape, r, cfg, dims, bnd):
+    """A 256-column tile on grids narrower than it: at 44 columns the second
+    TMA box of every plane lies wholly outside the grid (filled with zeros)
+    and the first is partial (a ragged last chunk of 4 columns); at 136 the
+    second box holds 8 columns.  FP32 rows are 16-byte multiples at both
+    widths (TMA); BF16 rows of 44 are not (plain-load producer)."""
+    check_configuration(cuda, tmp_path, dt, shape, r, cfg, dims, bnd)
 
 
 def sweep_cases():
