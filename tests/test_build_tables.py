@@ -42,6 +42,48 @@ def test_3d_configuration_fits_and_has_its_ring(inst):
         assert shape == 0 and r == 1  # the Jacobi sweep is the 7-point star
 
 
+@pytest.mark.parametrize("inst", instances_3d(), ids=lambda c: "-".join(map(str, c)))
+def test_3d_slot_layout(inst):
+    """The shared-memory slot layout of Stencil3DCfg, restated: every box's
+    TMA destination starts on a 128-byte boundary and its first column on a
+    16-byte one (for any column tile), each lane's vector reads are aligned
+    and inside the slot, the x-halo reads of lanes 0 and 31 stay inside their
+    box's row, and lane L's first column is tile origin + L*V."""
+    dt, shape, r, py, nw, s, rhs, dflt, zreg, v = inst
+    es = ES[dt]
+    hx = 16 // es
+    tx = 32 * v
+    nbox = 2 if tx + 2 * hx > 256 else 1
+    bw = (tx + 2 * hx) // nbox
+    rym = 1 if shape == 1 else r
+    yw = nw * py + 2 * rym
+    boxs = (bw * yw * es + 127) // 128 * 128 // es
+    slot = nbox * boxs
+    lpb = 32 // nbox
+    assert bw <= 256 and (bw * es) % 16 == 0 and (boxs * es) % 128 == 0
+
+    def col_off(lane):
+        return (lane // lpb) * boxs + (hx if lane // lpb == 0 else 0) + (lane % lpb) * v
+
+    for tile in range(3):
+        for b in range(nbox):
+            assert ((tile * tx - hx + b * bw) * es) % 16 == 0
+    for lane in range(32):
+        b = lane // lpb
+        assert -hx + b * bw + col_off(lane) - b * boxs == lane * v
+        for row in range(yw):
+            a = row * bw + col_off(lane)
+            assert 0 <= a and a + v <= slot
+            if (v * es) % 16 == 0:
+                assert (a * es) % 16 == 0
+    for row in range(yw):
+        for h in range(r):
+            left = row * bw + col_off(0) - 1 - h
+            right = row * bw + col_off(31) + v + h
+            assert row * bw <= left < (row + 1) * bw
+            assert (nbox - 1) * boxs + row * bw <= right < (nbox - 1) * boxs + (row + 1) * bw
+
+
 def test_3d_groups_have_exactly_one_default():
     groups = Counter((dt, shape, r, rhs) for (dt, shape, r, _, _, _, rhs, dflt, _, _)
                      in instances_3d() if dflt)
