@@ -238,12 +238,20 @@ _CPU_PROBE: dict = {}  # per workload: (seconds per row, cached inputs)
 
 
 def cpu_reference_rate(spec, budget_s: float, seed: int = 7):
-    """The reference's compiled Convolution<T> on the host cores: returns
-    (GCells/s, sample description, cores).  Runs whole grids until
-    ~budget_s, or a row slab of the grid when one grid takes longer."""
+    """The reference's compiled Convolution<T> (or 3D gold) on the host
+    cores: returns (GCells/s, sample description, cores, kind).  Runs whole
+    grids until ~budget_s, or a row slab of the grid when one grid takes
+    longer.  kind is "reference" when oracle/_ref was built from the
+    reference's sources, else "port": the oracle's C restatement of the same
+    loops (also OpenMP over rows) stands in for it."""
     import oracle
-    if not oracle.have_ref():
-        raise RuntimeError("oracle/_ref is not built")
+    use_ref = oracle.have_ref()
+    kind = "reference" if use_ref else "port"
+    if use_ref:
+        conv = oracle.ref_convolution
+    else:
+        def conv(a, m):
+            return oracle.conv2d(a, m, "zero")
     dt = np_dtype(spec["dtype"]) or np.float32
     n = spec["n"]
     g = np.random.Generator(np.random.PCG64(seed))
@@ -252,16 +260,30 @@ def cpu_reference_rate(spec, budget_s: float, seed: int = 7):
         # the reference gold for this stencil (v2::j3d7pt_gold / j3d13pt_gold /
         # poisson_gold), iterated with copy-back like its IT-step check
         cur = g.random((n, n, n), dtype=np.float32).astype(dt)
+        if use_ref:
+            def gold(a):
+                return oracle.ref_gold3d(spec["gold"], a)
+        elif spec["gold"] == "poisson":
+            def gold(a):
+                return oracle.poisson19(a, "gold")
+        else:
+            cube = cube3d(spec)
+            r = spec["r"]
+            taps = [(z - r, y - r, x - r, float(cube[z, y, x]))
+                    for z, y, x in zip(*np.nonzero(cube))]
+
+            def gold(a):
+                return oracle.taps3d(a, taps, "gold")
         t0 = time.perf_counter()
         done = 0
         while True:
-            cur = oracle.ref_gold3d(spec["gold"], cur)
+            cur = gold(cur)
             done += 1
             el = time.perf_counter() - t0
             if el >= budget_s or done >= spec["steps"]:
                 break
         sample = f"{done} of {spec['steps']} step(s) on the full {n}^3 grid"
-        return n ** 3 * done / el / 1e9, sample, cores
+        return n ** 3 * done / el / 1e9, sample, cores, kind
     c = coefficients(spec)
     if spec["kind"] == "star":
         r = spec["r"]
@@ -280,7 +302,7 @@ def cpu_reference_rate(spec, budget_s: float, seed: int = 7):
         rows = min(n, 256)
         slab = g.uniform(-1, 1, size=(rows, n)).astype(dt)
         t0 = time.perf_counter()
-        oracle.ref_convolution(slab, m)
+        conv(slab, m)
         _CPU_PROBE[key] = ((time.perf_counter() - t0) / rows, {})
     per_row, inputs = _CPU_PROBE[key]
     steps = spec["steps"]
@@ -294,7 +316,7 @@ def cpu_reference_rate(spec, budget_s: float, seed: int = 7):
         for _ in range(reps):
             cur = src
             for _ in range(steps):
-                cur = oracle.ref_convolution(cur, m)
+                cur = conv(cur, m)
         el = time.perf_counter() - t0
         cells = reps * n * n * steps
         sample = f"{reps} x full {n}x{n} grid x {steps} step(s)"
@@ -307,11 +329,11 @@ def cpu_reference_rate(spec, budget_s: float, seed: int = 7):
         t0 = time.perf_counter()
         cur = src
         for _ in range(steps):
-            cur = oracle.ref_convolution(cur, m)
+            cur = conv(cur, m)
         el = time.perf_counter() - t0
         cells = rows * n * steps
         sample = f"{rows}-row slab of the {n}x{n} grid x {steps} step(s)"
-    return cells / el / 1e9, sample, cores
+    return cells / el / 1e9, sample, cores, kind
 
 
 # ------------------------------------------------------------ reference arm --
@@ -379,13 +401,13 @@ def run_reference(args, spec, name):
     # 2020 steps about 3.5 minutes); the line's value is the median rate
     budget = max(0.1, min(10.0, 150.0 / max(1, n_steps)))
     rates = []
-    sample = cores = None
+    sample = cores = cpu_kind = None
     for i in range(n_steps):
         if spec["kind"] == "batched":
             cb = batched_cpu_baseline(spec, batch_sides(spec), budget)
-            rate, sample, cores = cb["value"], cb["sample"], cb["cores"]
+            rate, sample, cores, cpu_kind = cb["value"], cb["sample"], cb["cores"], cb["kind"]
         else:
-            rate, sample, cores = cpu_reference_rate(spec, budget, seed=i)
+            rate, sample, cores, cpu_kind = cpu_reference_rate(spec, budget, seed=i)
         if i >= args.warmup:
             rates.append(rate)
     value = statistics.median(rates) if rates else None
@@ -403,7 +425,7 @@ def run_reference(args, spec, name):
                        radius=spec["r"], steps_per_call=spec["steps"],
                        boundary=spec["boundary"]),
         "cpu_baseline": {"value": value, "unit": "GCells/s", "cores": cores,
-                         "kind": "reference", "sample": f"per step: {sample}"},
+                         "kind": cpu_kind, "sample": f"per step: {sample}"},
         "e2e": {"value": value, "unit": "GCells/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -541,8 +563,10 @@ def run_batched(args, spec, name):
 
 def batched_cpu_baseline(spec, sides, budget_s=10.0):
     """Reference Convolution<float> per grid, looped like the reference would
-    run one grid per invocation, on the host cores."""
+    run one grid per invocation, on the host cores (the oracle's restatement
+    of it when oracle/_ref is not built: kind "port")."""
     import oracle
+    use_ref = oracle.have_ref()
     g = np.random.Generator(np.random.PCG64(3))
     c = coefficients(spec)
     r = spec["r"]
@@ -559,13 +583,14 @@ def batched_cpu_baseline(spec, sides, budget_s=10.0):
     for h, w_ in sides:
         x = g.random((int(h), int(w_)), dtype=np.float32)
         for _ in range(spec["steps"]):
-            x = oracle.ref_convolution(x, m)
+            x = oracle.ref_convolution(x, m) if use_ref else oracle.conv2d(x, m, "zero")
         cells += int(h) * int(w_) * spec["steps"]
         if time.perf_counter() - t0 > budget_s:
             break
     el = time.perf_counter() - t0
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
-    return {"value": cells / el / 1e9, "unit": "GCells/s", "cores": cores, "kind": "reference",
+    return {"value": cells / el / 1e9, "unit": "GCells/s", "cores": cores,
+            "kind": "reference" if use_ref else "port",
             "sample": f"{cells // spec['steps']} cells of the batch x {spec['steps']} steps"}
 
 
@@ -1085,8 +1110,8 @@ def run_ssam(args, spec, name):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            rate, sample, cores = cpu_reference_rate(spec, budget_s=10.0)
-            cpu = {"value": rate, "unit": "GCells/s", "cores": cores, "kind": "reference",
+            rate, sample, cores, cpu_kind = cpu_reference_rate(spec, budget_s=10.0)
+            cpu = {"value": rate, "unit": "GCells/s", "cores": cores, "kind": cpu_kind,
                    "sample": sample}
         except Exception as exc:  # the GPU number stands without it
             cpu = {"value": None, "unit": "GCells/s", "cores": None, "kind": "reference",
