@@ -304,7 +304,8 @@ SSAM_API int ssam_autotune_jacobi3d(int64_t n, int nbatch, int sweep_dtype, void
  * (t: time steps fused in one launch; P: rows a thread, or the streaming
  * segment; V: columns a thread)
  * (a choice3d line without its last field means V = 4).  Writing such lines
- * by hand pins a configuration; load fails with SSAM_ERR_INVALID, naming the
+ * by hand pins a configuration (one that is not compiled into the library
+ * is kept but not used: calls fall back to a compiled default); load fails with SSAM_ERR_INVALID, naming the
  * count of malformed lines, when a line does not parse or a value is out of
  * range, after loading the good ones. */
 SSAM_API int ssam_autotune_save(const char* path);
