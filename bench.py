@@ -237,6 +237,28 @@ class ClockSampler:
 _CPU_PROBE: dict = {}  # per workload: (seconds per row, cached inputs)
 
 
+def host_threads() -> int:
+    """Threads the OpenMP loops of oracle/ and oracle/_ref run with: the
+    OMP_NUM_THREADS setting, else every core this process may use."""
+    env = os.environ.get("OMP_NUM_THREADS", "").split(",")[0].strip()
+    if env.isdigit() and int(env) > 0:
+        return int(env)
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+
+
+def cpu_model() -> str:
+    """The host CPU's model name (/proc/cpuinfo), for the cpu_baseline line."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
 def cpu_reference_rate(spec, budget_s: float, seed: int = 7):
     """The reference's compiled Convolution<T> (or 3D gold) on the host
     cores: returns (GCells/s, sample description, cores, kind).  Runs whole
@@ -255,7 +277,7 @@ def cpu_reference_rate(spec, budget_s: float, seed: int = 7):
     dt = np_dtype(spec["dtype"]) or np.float32
     n = spec["n"]
     g = np.random.Generator(np.random.PCG64(seed))
-    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    cores = host_threads()
     if spec["kind"] == "3d":
         # the reference gold for this stencil (v2::j3d7pt_gold / j3d13pt_gold /
         # poisson_gold), iterated with copy-back like its IT-step check
@@ -351,7 +373,8 @@ def poisson_cpu_baseline(f_np, sweeps_needed, budget_s=10.0):
         done += 4
     el = time.perf_counter() - t0
     per_sweep = el / done
-    return {"value": per_sweep * sweeps_needed, "unit": "s", "cores": 1, "kind": "port",
+    return {"value": per_sweep * sweeps_needed, "unit": "s", "cores": host_threads(),
+            "cpu_model": cpu_model(), "kind": "port",
             "sample": f"{done} FP64 Jacobi sweeps of the 8 x 128^3 problem in {el:.2f} s "
                       f"({f_np.size * done / el / 1e9:.3f} GCell-updates/s), extrapolated to "
                       f"the {sweeps_needed} sweeps the plain arm needed"}
@@ -425,7 +448,8 @@ def run_reference(args, spec, name):
                        radius=spec["r"], steps_per_call=spec["steps"],
                        boundary=spec["boundary"]),
         "cpu_baseline": {"value": value, "unit": "GCells/s", "cores": cores,
-                         "kind": cpu_kind, "sample": f"per step: {sample}"},
+                         "cpu_model": cpu_model(), "kind": cpu_kind,
+                         "sample": f"per step: {sample}"},
         "e2e": {"value": value, "unit": "GCells/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -588,9 +612,9 @@ def batched_cpu_baseline(spec, sides, budget_s=10.0):
         if time.perf_counter() - t0 > budget_s:
             break
     el = time.perf_counter() - t0
-    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    cores = host_threads()
     return {"value": cells / el / 1e9, "unit": "GCells/s", "cores": cores,
-            "kind": "reference" if use_ref else "port",
+            "cpu_model": cpu_model(), "kind": "reference" if use_ref else "port",
             "sample": f"{cells // spec['steps']} cells of the batch x {spec['steps']} steps"}
 
 
@@ -1112,7 +1136,7 @@ def run_ssam(args, spec, name):
         try:
             rate, sample, cores, cpu_kind = cpu_reference_rate(spec, budget_s=10.0)
             cpu = {"value": rate, "unit": "GCells/s", "cores": cores, "kind": cpu_kind,
-                   "sample": sample}
+                   "cpu_model": cpu_model(), "sample": sample}
         except Exception as exc:  # the GPU number stands without it
             cpu = {"value": None, "unit": "GCells/s", "cores": None, "kind": "reference",
                    "sample": f"unavailable: {exc}"}

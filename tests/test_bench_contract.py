@@ -32,7 +32,7 @@ def test_reference_arm_line():
     assert d["value"] > 0 and d["higher_is_better"] is True and d["steps"] == 1
     assert d["config"]["workload"] == "star1_f32_4096_copy"
     cb = d["cpu_baseline"]
-    assert cb["value"] == d["value"] and cb["cores"] >= 1 and cb["sample"]
+    assert cb["value"] == d["value"] and cb["cores"] >= 1 and cb["sample"] and cb["cpu_model"]
     assert cb["kind"] == ("reference" if oracle.have_ref() else "port")
     assert d["e2e"] == {"value": d["value"], "unit": "GCells/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
@@ -74,3 +74,10 @@ def test_cpu_rate_reference_or_port(monkeypatch, spec, built):
     rate, sample, cores, kind = bench.cpu_reference_rate(dict(spec), budget_s=0.2)
     assert rate > 0 and cores >= 1 and sample
     assert kind == ("reference" if built else "port")
+
+
+def test_host_threads_follows_omp_num_threads(monkeypatch):
+    monkeypatch.setenv("OMP_NUM_THREADS", "3")
+    assert bench.host_threads() == 3
+    monkeypatch.delenv("OMP_NUM_THREADS")
+    assert bench.host_threads() >= 1
