@@ -81,3 +81,10 @@ def test_host_threads_follows_omp_num_threads(monkeypatch):
     assert bench.host_threads() == 3
     monkeypatch.delenv("OMP_NUM_THREADS")
     assert bench.host_threads() >= 1
+
+
+def test_poisson_cpu_baseline_small():
+    from ssam_b200.workloads import gaussian_rhs
+    cb = bench.poisson_cpu_baseline(gaussian_rhs(1, 16, 5), 1000, budget_s=0.2)
+    assert cb["value"] > 0 and cb["unit"] == "s" and cb["kind"] == "port"
+    assert cb["cores"] == bench.host_threads() and cb["cpu_model"] and "sweeps" in cb["sample"]
