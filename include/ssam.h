@@ -403,7 +403,8 @@ SSAM_API int ssam_poisson_solve_learned(const double* f, double* u, int n, int n
                                         const ssam_poisson_options* opt, void* cnn,
                                         ssam_poisson_stats* stats, void* stream);
 
-/* ||f - A u||_2 / ||f||_2 per right-hand side, in FP64 (`rel` is host, nbatch). */
+/* ||f - A u||_2 / ||f||_2 per right-hand side, in FP64 (`rel` is host, nbatch);
+ * ||f - A u||_2 itself where f = 0. */
 SSAM_API int ssam_poisson_residual(const double* f, const double* u, int n, int nbatch,
                                    double* rel, void* stream);
 

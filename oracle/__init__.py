@@ -208,12 +208,14 @@ def jacobi7(rhs: np.ndarray, u: np.ndarray, sweeps: int) -> np.ndarray:
 
 
 def residual7(f: np.ndarray, u: np.ndarray):
-    """(r, rel) with r = f - A u and rel = ||r|| / ||f|| per right-hand side."""
+    """(r, rel) with r = f - A u and rel = ||r|| / ||f|| per right-hand side
+    (||r|| itself where f = 0, as the library's ssam_poisson_residual)."""
     f = np.ascontiguousarray(f, np.float64)
     u = np.ascontiguousarray(u, np.float64)
     nb, n = f.shape[0], f.shape[1]
     r = np.empty_like(f)
     norms = np.zeros(2 * nb)
     lib().ssam_oracle_residual7_f64(_ptr(f), _ptr(u), _ptr(r), _i64(n), _i64(nb), _ptr(norms))
-    return r, np.sqrt(norms[0::2] / norms[1::2])
+    rr, ff = norms[0::2], norms[1::2]
+    return r, np.sqrt(np.where(ff > 0, rr / np.where(ff > 0, ff, 1.0), rr))
 

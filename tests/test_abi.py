@@ -14,7 +14,8 @@ HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))
 
 
 def declared_functions():
-    text = open(HEADER).read()
+    with open(HEADER) as f:
+        text = f.read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return re.findall(r"SSAM_API\s+[\w\s\*]+?\b(ssam_\w+)\s*\(", text)
 

@@ -134,7 +134,9 @@ def test_poisson_residual_identity_and_jacobi_fixed_point():
     g = rng(11)
     u = g.standard_normal((2, 9, 9, 9))
     # r = 0 - A u  =>  f := A u makes u the exact discrete solution
-    r, _ = oracle.residual7(np.zeros_like(u), u)
+    r, rel0 = oracle.residual7(np.zeros_like(u), u)
+    # f = 0: the residual norm itself (the library's rule), not a division by 0
+    np.testing.assert_allclose(rel0, np.sqrt((r.reshape(2, -1) ** 2).sum(axis=1)), rtol=1e-12)
     f = -r
     _, rel = oracle.residual7(f, u)
     assert rel.max() < 1e-13
