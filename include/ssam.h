@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define SSAM_ABI_VERSION 1
+#define SSAM_ABI_VERSION 2
 
 /* Exported symbols (the library is built with hidden visibility). */
 #if defined(__GNUC__)
@@ -269,17 +269,22 @@ typedef struct ssam_tune3d_report {
                          registers (shared memory carries the halos only) */
   int columns_per_thread; /* V: the tile is 32*V columns wide */
   int candidates;     /* configurations timed */
-  double ms_per_step; /* best measured time of one launch (ms) */
+  double ms_per_step; /* best measured time per step: one launch's time / fused_steps (ms) */
+  int fused_steps;    /* time steps one launch of the chosen configuration applies (1 or 2) */
 } ssam_tune3d_report;
 
 /*
  * Times every compiled configuration of this 3D stencil (rows per warp,
- * consumer warps, shared-memory ring depth) for one step on the caller's
- * buffers (dst is overwritten) and stores the fastest for the grid's size
- * class (log2 of nx, ny, nz); later ssam_stencil3d / _host calls on grids of
- * that class use it (cached step graphs are re-captured).  The reference
- * fixes these per GPU model (BLOCK_SIZE / PROCESS_DATA_COUNT chosen with
- * IsTeslaV100(), tmp3d7pt-v2.cu:341-387).  Synchronous.  `report` may be NULL.
+ * consumer warps, shared-memory ring depth), both the single-step kernels and
+ * those that fuse two time steps in one z-march, on the caller's buffers (dst
+ * is overwritten), and stores for the grid's size class (log2 of nx, ny, nz)
+ * the fastest of each and the temporal depth (1 or 2 steps a launch) with
+ * the lower time per step; later ssam_stencil3d / _host calls on grids of
+ * that class use them (cached step graphs are re-captured).  The reference
+ * fixes these per GPU model (BLOCK_SIZE / PROCESS_DATA_COUNT /
+ * ITERATIVE_COUNT chosen with IsTeslaV100(), tmp3d7pt-v2.cu:341-387).
+ * Synchronous.  `report` describes the configuration of the chosen depth and
+ * may be NULL.
  */
 SSAM_API int ssam_autotune_stencil3d(const void* src, void* dst, int64_t nx, int64_t ny,
                                      int64_t nz, int dtype, int shape, int radius,
@@ -300,10 +305,13 @@ SSAM_API int ssam_autotune_jacobi3d(int64_t n, int nbatch, int sweep_dtype, void
  * autotuners.  The file is text, one choice a line ('#' starts a comment):
  *   choice   dtype rl rr rt rb star t log2w log2h P warps V
  *   depth    dtype rl rr rt rb star log2w log2h t
- *   choice3d dtype shape radius rhs log2nx log2ny log2(nz*nbatch) PY NW S zreg V
+ *   choice3d dtype shape radius rhs log2nx log2ny log2(nz*nbatch) PY NW S zreg V t
+ *   depth3d  dtype shape radius log2nx log2ny log2nz t
  * (t: time steps fused in one launch; P: rows a thread, or the streaming
- * segment; V: columns a thread)
- * (a choice3d line without its last field means V = 4).  Writing such lines
+ * segment; V: columns a thread; shape: 0 star, 1 19-point)
+ * (a choice3d line without its last field means t = 1, without its last two
+ * V = 4 and t = 1; with no depth3d line for a size class, multi-step 3D runs
+ * take one step a launch).  Writing such lines
  * by hand pins a configuration (one that is not compiled into the library
  * is kept but not used: calls fall back to a compiled default); load fails with SSAM_ERR_INVALID, naming the
  * count of malformed lines, when a line does not parse or a value is out of
@@ -329,9 +337,16 @@ SSAM_API int ssam_autotune_clear(void);
  * digits = offset + r (tmp3d7pt-v2.cu:9-15).  Entries outside the shape's
  * pattern are ignored.  Supported: SSAM_STAR3D r = 1, 2 and SSAM_POISSON19.
  * boundary: ZERO or COPY (the reference golds' interior with the ring kept).
- * steps > 1 chain through a stream-ordered scratch grid; unless the stream is
- * already being captured, the whole chain is captured once into a CUDA graph
+ * steps > 1: one step a launch, or -- where ssam_autotune_stencil3d measured
+ * it faster for the size class, or a depth3d line pins it -- launches that
+ * each fuse two time steps in one z-march (temporal blocking, like the
+ * reference's ITERATIVE_COUNT, tmp3d7pt-v2.cu:124-170; FP32/BF16 all three
+ * shapes, FP64 r = 1) plus a single step for an odd count; they chain
+ * through a stream-ordered scratch grid and, unless the stream is already
+ * being captured, the whole chain is captured once into a CUDA graph
  * (cached per pointers/sizes/coefficients) and replayed on later calls.
+ * Intermediate steps are rounded to the storage type, as a chain of single
+ * steps stores them.
  */
 SSAM_API int ssam_stencil3d(const void* src, void* dst, int64_t nx, int64_t ny, int64_t nz,
                             int dtype, int shape, int radius, const double* coeffs,

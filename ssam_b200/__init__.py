@@ -385,7 +385,7 @@ class Tune3DReport(ctypes.Structure):
     _fields_ = [("rows_per_warp", ctypes.c_int), ("consumer_warps", ctypes.c_int),
                 ("ring_slots", ctypes.c_int), ("registers_z", ctypes.c_int),
                 ("columns_per_thread", ctypes.c_int), ("candidates", ctypes.c_int),
-                ("ms_per_step", ctypes.c_double)]
+                ("ms_per_step", ctypes.c_double), ("fused_steps", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -117,6 +117,32 @@ def instances_3d():
     return out
 
 
+def instances_3d_t2():
+    """(dtype, shape, r, PY, NW, S, V, default) of every compiled 3D
+    configuration that applies two time steps per launch (stencil3d_t2.cuh):
+    shape 0 = star (r = 1: 7-pt, r = 2: 13-pt), 1 = the 19-point operator.
+    The first of each group is the default.  Limits (static_asserts of the
+    kernel): 2*R*(PY + 2*EY) <= 32 x-halo values a warp (EY = 1 for the
+    19-point operator, else 0), 2R staged halo columns (FP64 holds 2: r = 1
+    only), PY >= R, ring slots S >= 2R + 2."""
+    cfg = {
+        "f32": {(0, 1): [(4, 8, 6, 4), (2, 8, 6, 8), (4, 7, 6, 4), (6, 7, 6, 4), (2, 8, 4, 8)],
+                (0, 2): [(2, 8, 8, 4), (4, 7, 8, 4)],
+                (1, 1): [(2, 8, 6, 4), (4, 7, 6, 4)]},
+        "bf16": {(0, 1): [(2, 8, 6, 8), (4, 7, 6, 8), (4, 8, 6, 4)],
+                 (0, 2): [(2, 8, 8, 4), (4, 7, 8, 4)],
+                 (1, 1): [(2, 8, 6, 8), (4, 7, 6, 4)]},
+        "f64": {(0, 1): [(2, 8, 6, 4), (4, 7, 6, 4)],
+                (1, 1): [(2, 8, 6, 4)]},
+    }
+    out = []
+    for dt, groups in cfg.items():
+        for (shape, r), lst in groups.items():
+            for i, (py, nw, s_, v) in enumerate(lst):
+                out.append((dt, shape, r, py, nw, s_, v, i == 0))
+    return out
+
+
 def rowloop_instances():
     """(dtype, rl, rr, V) of every compiled row-loop 2D kernel (square filters
     of width FW = rl + rr + 1 >= 7: box r = 3..5 and the wider correlations;
@@ -201,6 +227,28 @@ def _gen_units(chunk: int = 6):
                     f"static Register3D<{DTYPES[dt]}, {sh}, {r}, {py}, {nw}, {s}, "
                     f"{'true' if rhs else 'false'}, {'true' if dflt else 'false'}, "
                     f"{'true' if zreg else 'false'}, {v}> reg3_{tag};")
+            lines.append("}  // namespace ssam")
+            text = "\n".join(lines) + "\n"
+            path = os.path.join(BUILD, "gen", name)
+            if not os.path.exists(path) or open(path).read() != text:
+                with open(path, "w") as f:
+                    f.write(text)
+            units.append(path)
+    by_dt = {}
+    for inst in instances_3d_t2():
+        by_dt.setdefault(inst[0], []).append(inst)
+    for dt, lst in by_dt.items():
+        for c in range(0, len(lst), 2):
+            part = lst[c:c + 2]
+            name = f"inst3dt_{dt}_{c // 2:02d}.cu"
+            lines = ["// generated by ssam_b200/build.py -- do not edit",
+                     '#include "../../csrc/stencil3d_launch.cuh"', "namespace ssam {"]
+            for (_, shape, r, py, nw, s_, v, dflt) in part:
+                sh = "SH3_POISSON19" if shape else "SH3_STAR"
+                lines.append(
+                    f"static Register3D<{DTYPES[dt]}, {sh}, {r}, {py}, {nw}, {s_}, false, "
+                    f"{'true' if dflt else 'false'}, false, {v}, 2> "
+                    f"reg3t_{shape}_{r}_{py}_{nw}_{s_}_{v};")
             lines.append("}  // namespace ssam")
             text = "\n".join(lines) + "\n"
             path = os.path.join(BUILD, "gen", name)

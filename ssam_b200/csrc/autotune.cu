@@ -269,8 +269,14 @@ extern "C" int ssam_autotune_save(const char* path) {
   }
   tune3d_for_each(
       [](const int* k, const int* v, void* u) {
-        fprintf((FILE*)u, "choice3d %d %d %d %d %d %d %d %d %d %d %d %d\n", k[0], k[1], k[2],
-                k[3], k[4], k[5], k[6], v[0], v[1], v[2], v[3], v[4]);
+        fprintf((FILE*)u, "choice3d %d %d %d %d %d %d %d %d %d %d %d %d %d\n", k[0], k[1],
+                k[2], k[3], k[4], k[5], k[6], v[0], v[1], v[2], v[3], v[4], k[7]);
+      },
+      f);
+  depth3d_for_each(
+      [](const int* k, int d, void* u) {
+        fprintf((FILE*)u, "depth3d %d %d %d %d %d %d %d\n", k[0], k[1], k[2], k[3], k[4], k[5],
+                d);
       },
       f);
   fclose(f);
@@ -293,16 +299,23 @@ extern "C" int ssam_autotune_load(const char* path) {
       if (a[9] < 1 || a[10] < 1 || a[10] > 8 || a[11] < 1) { ++bad; continue; }
       c.choices[TuneKey{a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8]}] =
           TuneChoice{a[9], a[10], a[11]};
-    } else if (int n3 = sscanf(line, "choice3d %d %d %d %d %d %d %d %d %d %d %d %d", &a[0],
+    } else if (int n3 = sscanf(line, "choice3d %d %d %d %d %d %d %d %d %d %d %d %d %d", &a[0],
                                &a[1], &a[2], &a[3], &a[4], &a[5], &a[6], &a[7], &a[8], &a[9],
-                               &a[10], &a[11]);
-               n3 == 11 || n3 == 12) {
-      if (n3 == 11) a[11] = 4;  // lines written before the V field: 4 columns a thread
-      if (a[7] < 1 || a[8] < 1 || a[9] < 1 || a[10] < 0 || a[10] > 1 || a[11] < 1) {
+                               &a[10], &a[11], &a[12]);
+               n3 >= 11 && n3 <= 13) {
+      if (n3 < 12) a[11] = 4;  // lines written before the V field: 4 columns a thread
+      if (n3 < 13) a[12] = 1;  // lines written before the steps field: one step a launch
+      if (a[7] < 1 || a[8] < 1 || a[9] < 1 || a[10] < 0 || a[10] > 1 || a[11] < 1 ||
+          a[12] < 1 || a[12] > 2) {
         ++bad;
         continue;
       }
-      tune3d_store(a, a + 7);
+      const int key[8] = {a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[12]};
+      tune3d_store(key, a + 7);
+    } else if (sscanf(line, "depth3d %d %d %d %d %d %d %d", &a[0], &a[1], &a[2], &a[3], &a[4],
+                      &a[5], &a[6]) == 7) {
+      if (a[6] < 1 || a[6] > 2) { ++bad; continue; }
+      depth3d_store(a, a[6]);
     } else if (sscanf(line, "depth %d %d %d %d %d %d %d %d %d", &a[0], &a[1], &a[2], &a[3],
                       &a[4], &a[5], &a[6], &a[7], &a[8]) == 9) {
       if (a[8] < 1) { ++bad; continue; }

@@ -23,9 +23,13 @@ int tune_depth_2d(int dtype, int rl, int rr, int rt, int rb, int star, int64_t w
                   int64_t h, int steps);
 
 // The 3D autotuner's measured choices (stencil3d.cu): key = (dtype, shape,
-// radius, rhs, log2 nx, log2 ny, log2 nz*nbatch), value = (PY, NW, S, zreg, V).
-void tune3d_for_each(void (*cb)(const int key[7], const int val[5], void*), void* user);
-void tune3d_store(const int key[7], const int val[5]);
+// radius, rhs, log2 nx, log2 ny, log2 nz*nbatch, steps per launch), value =
+// (PY, NW, S, zreg, V); and the temporal depth of multi-step runs, key =
+// (dtype, shape, radius, log2 nx, log2 ny, log2 nz), value = steps per launch.
+void tune3d_for_each(void (*cb)(const int key[8], const int val[5], void*), void* user);
+void tune3d_store(const int key[8], const int val[5]);
+void depth3d_for_each(void (*cb)(const int key[6], int depth, void*), void* user);
+void depth3d_store(const int key[6], int depth);
 void tune3d_clear();
 
 }  // namespace ssam

@@ -56,7 +56,7 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() { return encode_fn(); }
 
 // ------------------------------------------------- configuration table --
 
-using Key3D = std::tuple<int, int, int, int>;  // dtype, shape, radius, rhs
+using Key3D = std::tuple<int, int, int, int, int>;  // dtype, shape, radius, rhs, steps/launch
 
 static std::map<Key3D, std::vector<Cand3D>>& table_3d() {
   static std::map<Key3D, std::vector<Cand3D>> t;
@@ -64,20 +64,24 @@ static std::map<Key3D, std::vector<Cand3D>>& table_3d() {
 }
 
 void register_3d(int dtype, int shape, int r, bool rhs, const Cand3D& c) {
-  table_3d()[Key3D{dtype, shape, r, rhs ? 1 : 0}].push_back(c);
+  table_3d()[Key3D{dtype, shape, r, rhs ? 1 : 0, c.t}].push_back(c);
 }
 
-static const std::vector<Cand3D>* cands_3d(int dtype, int shape, int r, bool rhs) {
-  auto it = table_3d().find(Key3D{dtype, shape, r, rhs ? 1 : 0});
+static const std::vector<Cand3D>* cands_3d(int dtype, int shape, int r, bool rhs, int t = 1) {
+  auto it = table_3d().find(Key3D{dtype, shape, r, rhs ? 1 : 0, t});
   return it == table_3d().end() || it->second.empty() ? nullptr : &it->second;
 }
 
-// Measured choices: (dtype, shape, radius, rhs, log2 nx, log2 ny, log2 nz*nb)
-// -> (PY, NW, S, zreg, V).
-using Tune3DKey = std::tuple<int, int, int, int, int, int, int>;
+// Measured choices: (dtype, shape, radius, rhs, log2 nx, log2 ny, log2 nz*nb,
+// steps per launch) -> (PY, NW, S, zreg, V); and the measured temporal depth
+// (1 or 2 steps a launch) of multi-step runs per (dtype, shape, radius,
+// log2 nx, log2 ny, log2 nz).
+using Tune3DKey = std::tuple<int, int, int, int, int, int, int, int>;
 using Tune3DVal = std::tuple<int, int, int, int, int>;
+using Depth3DKey = std::tuple<int, int, int, int, int, int>;
 static std::mutex g_tune3_mu;
 static std::map<Tune3DKey, Tune3DVal> g_tune3;
+static std::map<Depth3DKey, int> g_depth3;
 
 static int log2_floor(int64_t v) {
   int b = 0;
@@ -89,20 +93,24 @@ static int log2_floor(int64_t v) {
 }
 
 static Tune3DKey tune3_key(int dtype, int shape, int r, bool rhs, int64_t nx, int64_t ny,
-                           int64_t nzb) {
+                           int64_t nzb, int t = 1) {
   return Tune3DKey{dtype, shape, r, rhs ? 1 : 0, log2_floor(nx), log2_floor(ny),
-                   log2_floor(nzb)};
+                   log2_floor(nzb), t};
 }
 
-// The configuration for one launch: the measured one for this size class if
-// any, else the default.
+static Depth3DKey depth3_key(int dtype, int shape, int r, int64_t nx, int64_t ny, int64_t nz) {
+  return Depth3DKey{dtype, shape, r, log2_floor(nx), log2_floor(ny), log2_floor(nz)};
+}
+
+// The configuration for one launch of `t` steps: the measured one for this
+// size class if any, else the default (NULL if none is compiled).
 static const Cand3D* pick_3d(int dtype, int shape, int r, bool rhs, int64_t nx, int64_t ny,
-                             int64_t nzb) {
-  const std::vector<Cand3D>* cs = cands_3d(dtype, shape, r, rhs);
+                             int64_t nzb, int t = 1) {
+  const std::vector<Cand3D>* cs = cands_3d(dtype, shape, r, rhs, t);
   if (!cs) return nullptr;
   {
     std::lock_guard<std::mutex> g(g_tune3_mu);
-    auto it = g_tune3.find(tune3_key(dtype, shape, r, rhs, nx, ny, nzb));
+    auto it = g_tune3.find(tune3_key(dtype, shape, r, rhs, nx, ny, nzb, t));
     if (it != g_tune3.end())
       for (const Cand3D& c : *cs)
         if (Tune3DVal{c.py, c.nw, c.s, c.zreg, c.v} == it->second) return &c;
@@ -112,27 +120,54 @@ static const Cand3D* pick_3d(int dtype, int shape, int r, bool rhs, int64_t nx, 
   return &cs->front();
 }
 
-void tune3d_for_each(void (*cb)(const int key[7], const int val[5], void*), void* user) {
+// Steps per launch of a multi-step run: the measured depth of the size class
+// if any, else 1 (the single-step kernels measured faster per step than the
+// two-step ones at 512^3 on a B200; the autotuner decides per size class).
+static int depth_3d(int dtype, int shape, int r, int64_t nx, int64_t ny, int64_t nz) {
+  {
+    std::lock_guard<std::mutex> g(g_tune3_mu);
+    auto it = g_depth3.find(depth3_key(dtype, shape, r, nx, ny, nz));
+    if (it != g_depth3.end()) return it->second;
+  }
+  return 1;
+}
+
+void tune3d_for_each(void (*cb)(const int key[8], const int val[5], void*), void* user) {
   std::lock_guard<std::mutex> g(g_tune3_mu);
   for (auto& kv : g_tune3) {
-    const int k[7] = {std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first),
+    const int k[8] = {std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first),
                       std::get<3>(kv.first), std::get<4>(kv.first), std::get<5>(kv.first),
-                      std::get<6>(kv.first)};
+                      std::get<6>(kv.first), std::get<7>(kv.first)};
     const int v[5] = {std::get<0>(kv.second), std::get<1>(kv.second), std::get<2>(kv.second),
                       std::get<3>(kv.second), std::get<4>(kv.second)};
     cb(k, v, user);
   }
 }
 
-void tune3d_store(const int key[7], const int val[5]) {
+void depth3d_for_each(void (*cb)(const int key[6], int depth, void*), void* user) {
   std::lock_guard<std::mutex> g(g_tune3_mu);
-  g_tune3[Tune3DKey{key[0], key[1], key[2], key[3], key[4], key[5], key[6]}] =
+  for (auto& kv : g_depth3) {
+    const int k[6] = {std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first),
+                      std::get<3>(kv.first), std::get<4>(kv.first), std::get<5>(kv.first)};
+    cb(k, kv.second, user);
+  }
+}
+
+void tune3d_store(const int key[8], const int val[5]) {
+  std::lock_guard<std::mutex> g(g_tune3_mu);
+  g_tune3[Tune3DKey{key[0], key[1], key[2], key[3], key[4], key[5], key[6], key[7]}] =
       Tune3DVal{val[0], val[1], val[2], val[3], val[4]};
+}
+
+void depth3d_store(const int key[6], int depth) {
+  std::lock_guard<std::mutex> g(g_tune3_mu);
+  g_depth3[Depth3DKey{key[0], key[1], key[2], key[3], key[4], key[5]}] = depth;
 }
 
 void tune3d_clear() {
   std::lock_guard<std::mutex> g(g_tune3_mu);
   g_tune3.clear();
+  g_depth3.clear();
 }
 
 static const char* kNo3D =
@@ -147,12 +182,15 @@ struct GraphKey {
   int64_t nx, ny, nz;
   int dtype, shape, r, steps, boundary;
   std::vector<double> coef;
-  LaunchFn3D fn;  // the configuration captured (a new measured choice recaptures)
+  // the configurations captured (a new measured choice recaptures): fn2 runs
+  // two steps a launch (NULL: single steps only), fn1 the remaining step
+  LaunchFn3D fn1, fn2;
   bool operator<(const GraphKey& o) const {
-    return std::tie(src, dst, nx, ny, nz, dtype, shape, r, steps, boundary, coef, fn) <
+    return std::tie(src, dst, nx, ny, nz, dtype, shape, r, steps, boundary, coef, fn1, fn2) <
            std::tie(o.src, o.dst, o.nx, o.ny, o.nz, o.dtype, o.shape, o.r, o.steps,
-                    o.boundary, o.coef, o.fn);
+                    o.boundary, o.coef, o.fn1, o.fn2);
   }
+  int launches() const { return fn2 ? steps / 2 + steps % 2 : steps; }
 };
 
 struct GraphEntry {
@@ -186,14 +224,16 @@ static std::map<GraphKey, GraphEntry> g_graphs;
 static uint64_t g_graph_clock = 0;
 static const size_t kMaxGraphs = 8;
 
-// Enqueues the launch chain src -> (scratch <-> dst) ... -> dst.
-static int enqueue_chain_3d(LaunchFn3D fn, const GraphKey& k, void* scratch,
-                            cudaStream_t s) {
+// Enqueues the launch chain src -> (scratch <-> dst) ... -> dst: steps/2
+// two-step launches of fn2 (when set) and the remaining single steps of fn1.
+static int enqueue_chain_3d(const GraphKey& k, void* scratch, cudaStream_t s) {
+  const int nl = k.launches();
+  const int n2 = k.fn2 ? k.steps / 2 : 0;
   const void* in = k.src;
-  for (int i = 0; i < k.steps; ++i) {
-    void* out = ((k.steps - 1 - i) % 2 == 0) ? k.dst : scratch;
+  for (int i = 0; i < nl; ++i) {
+    void* out = ((nl - 1 - i) % 2 == 0) ? k.dst : scratch;
     Launch3D a{in, out, k.nx, k.ny, k.nz, 1, nullptr, 0.0, k.coef.data(), k.boundary, s, false};
-    int st = fn(a);
+    int st = (i < n2 ? k.fn2 : k.fn1)(a);
     if (st != SSAM_OK) return st;
     in = out;
   }
@@ -205,11 +245,16 @@ int run_3d(const void* src, void* dst, int64_t nx, int64_t ny, int64_t nz, int d
            cudaStream_t stream) {
   const Cand3D* c = pick_3d(dtype, shape, r, false, nx, ny, nz);
   if (!c) return fail(SSAM_ERR_UNSUPPORTED, kNo3D);
-  LaunchFn3D fn = c->fn;
+  LaunchFn3D fn2 = nullptr;
+  if (steps >= 2 && depth_3d(dtype, shape, r, nx, ny, nz) == 2) {
+    const Cand3D* c2 = pick_3d(dtype, shape, r, false, nx, ny, nz, 2);
+    if (c2) fn2 = c2->fn;
+  }
   const int f = 2 * r + 1;
   GraphKey k{src, dst, nx, ny, nz, dtype, shape, r, steps, boundary,
-             std::vector<double>(coef, coef + f * f * f), fn};
-  if (steps == 1) return enqueue_chain_3d(fn, k, nullptr, stream);
+             std::vector<double>(coef, coef + f * f * f), c->fn, fn2};
+  const int nl = k.launches();
+  if (nl == 1) return enqueue_chain_3d(k, nullptr, stream);
 
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   SSAM_CUDA_TRY(cudaStreamIsCapturing(stream, &cap));
@@ -219,7 +264,7 @@ int run_3d(const void* src, void* dst, int64_t nx, int64_t ny, int64_t nz, int d
     void* scratch = nullptr;
     int st = scratch_alloc(&scratch, bytes, stream);
     if (st != SSAM_OK) return st;
-    st = enqueue_chain_3d(fn, k, scratch, stream);
+    st = enqueue_chain_3d(k, scratch, stream);
     scratch_free(scratch, stream);
     return st;
   }
@@ -248,15 +293,18 @@ int run_3d(const void* src, void* dst, int64_t nx, int64_t ny, int64_t nz, int d
     int st = scratch_alloc(&e.scratch, bytes, stream);
     if (st != SSAM_OK) return st;
     SSAM_CUDA_TRY(cudaStreamSynchronize(stream));
-    Launch3D prep{k.src, k.dst, k.nx, k.ny, k.nz, 1, nullptr, 0.0, k.coef.data(), k.boundary,
-                  stream, true};
-    st = fn(prep);
-    if (st != SSAM_OK) return st;
+    for (LaunchFn3D fn : {k.fn1, k.fn2}) {
+      if (!fn) continue;
+      Launch3D prep{k.src, k.dst, k.nx, k.ny, k.nz, 1, nullptr, 0.0, k.coef.data(), k.boundary,
+                    stream, true};
+      st = fn(prep);
+      if (st != SSAM_OK) return st;
+    }
     cudaStream_t cs = nullptr;
     SSAM_CUDA_TRY(capture_stream(&cs));
     cudaGraph_t graph = nullptr;
     SSAM_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    st = enqueue_chain_3d(fn, k, e.scratch, cs);
+    st = enqueue_chain_3d(k, e.scratch, cs);
     cudaError_t ce = cudaStreamEndCapture(cs, &graph);
     if (st != SSAM_OK || ce != cudaSuccess) {
       if (graph) cudaGraphDestroy(graph);
@@ -269,7 +317,7 @@ int run_3d(const void* src, void* dst, int64_t nx, int64_t ny, int64_t nz, int d
       scratch_free(e.scratch, stream);
       return fail_cuda(ce, "cudaGraphInstantiate");
     }
-    e.launches = steps;
+    e.launches = nl;
     it = g_graphs.emplace(k, e).first;
   }
   it->second.last_use = ++g_graph_clock;
@@ -342,9 +390,9 @@ static int time_3d(const Cand3D& c, const Launch3D& a, cudaEvent_t e0, cudaEvent
 }
 
 // Times every configuration in `cs` with launch `a` (its fn ignored) and
-// stores the fastest under `key`.
+// stores the fastest under `key`; *best / *best_ms / *timed describe it.
 static int tune_3d(const std::vector<Cand3D>& cs, const Launch3D& a, const Tune3DKey& key,
-                   ssam_tune3d_report* report) {
+                   const Cand3D** best_out, double* best_ms_out, int* timed_out) {
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   SSAM_CUDA_TRY(cudaEventCreate(&e0));
   cudaError_t ce = cudaEventCreate(&e1);
@@ -380,16 +428,23 @@ static int tune_3d(const std::vector<Cand3D>& cs, const Launch3D& a, const Tune3
     std::lock_guard<std::mutex> g(g_tune3_mu);
     g_tune3[key] = Tune3DVal{best->py, best->nw, best->s, best->zreg, best->v};
   }
-  if (report) {
-    report->rows_per_warp = best->py;
-    report->consumer_warps = best->nw;
-    report->ring_slots = best->s;
-    report->registers_z = best->zreg;
-    report->columns_per_thread = best->v;
-    report->candidates = timed;
-    report->ms_per_step = best_ms;
-  }
+  *best_out = best;
+  *best_ms_out = best_ms;
+  *timed_out = timed;
   return SSAM_OK;
+}
+
+static void fill_report(ssam_tune3d_report* report, const Cand3D* c, double ms_per_step,
+                        int timed) {
+  if (!report) return;
+  report->rows_per_warp = c->py;
+  report->consumer_warps = c->nw;
+  report->ring_slots = c->s;
+  report->registers_z = c->zreg;
+  report->columns_per_thread = c->v;
+  report->candidates = timed;
+  report->ms_per_step = ms_per_step;
+  report->fused_steps = c->t;
 }
 
 }  // namespace ssam
@@ -407,7 +462,37 @@ extern "C" int ssam_autotune_stencil3d(const void* src, void* dst, int64_t nx, i
   if (!cs) return fail(SSAM_ERR_UNSUPPORTED, kNo3D);
   Launch3D a{src, dst, nx, ny, nz, 1, nullptr, 0.0, coeffs, boundary, (cudaStream_t)stream,
              false};
-  return tune_3d(*cs, a, tune3_key(dtype, sh, radius, false, nx, ny, nz), report);
+  const Cand3D* b1 = nullptr;
+  double ms1 = 0;
+  int n1 = 0;
+  st = tune_3d(*cs, a, tune3_key(dtype, sh, radius, false, nx, ny, nz), &b1, &ms1, &n1);
+  if (st != SSAM_OK) return st;
+  // two steps a launch, kept when its time per step beats one step a launch
+  int depth = 1;
+  const Cand3D* best = b1;
+  double ms = ms1;
+  int timed = n1;
+  const std::vector<Cand3D>* cs2 = cands_3d(dtype, sh, radius, false, 2);
+  if (cs2) {
+    const Cand3D* b2 = nullptr;
+    double ms2 = 0;
+    int n2 = 0;
+    st = tune_3d(*cs2, a, tune3_key(dtype, sh, radius, false, nx, ny, nz, 2), &b2, &ms2, &n2);
+    if (st != SSAM_OK) return st;
+    timed += n2;
+    if (ms2 / 2 < ms1) {
+      depth = 2;
+      best = b2;
+      ms = ms2 / 2;
+    }
+  }
+  const Depth3DKey dk = depth3_key(dtype, sh, radius, nx, ny, nz);
+  {
+    std::lock_guard<std::mutex> g(g_tune3_mu);
+    g_depth3[dk] = depth;
+  }
+  fill_report(report, best, ms, timed);
+  return SSAM_OK;
 }
 
 extern "C" int ssam_autotune_jacobi3d(int64_t n, int nbatch, int sweep_dtype, void* stream,
@@ -435,7 +520,12 @@ extern "C" int ssam_autotune_jacobi3d(int64_t n, int nbatch, int sweep_dtype, vo
     for (int k : {4, 10, 12, 14, 16, 22}) cube[k] = 1.0 / 6.0;
     Launch3D a{buf[0], buf[1], n, n, n, nbatch, buf[2], 1.0 / 6.0, cube, SSAM_BOUNDARY_ZERO,
                s, false};
-    st = tune_3d(*cs, a, tune3_key(sweep_dtype, SH3_STAR, 1, true, n, n, n * nbatch), report);
+    const Cand3D* best = nullptr;
+    double ms = 0;
+    int timed = 0;
+    st = tune_3d(*cs, a, tune3_key(sweep_dtype, SH3_STAR, 1, true, n, n, n * nbatch), &best,
+                 &ms, &timed);
+    if (st == SSAM_OK) fill_report(report, best, ms, timed);
   }
   for (int i = 0; i < 3; ++i) scratch_free(buf[i], s);
   return st;

@@ -241,26 +241,29 @@ __device__ __forceinline__ Seg3D item_seg(int64_t it, const Work3D& w) {
 }
 
 // The producer warp of a 3D CTA: stages every plane of every work item of
-// this CTA -- planes za-R .. zb+R-1 of the item's column tile, halos included
-// -- into the ring of S slots, in order.  A slot is reused once the consumer
-// warps have released its previous plane (empty barrier); a TMA copy signals
-// `full` by bytes, the plain-load path by 32 arrivals.  Every wait is
+// this CTA -- planes za-ZR .. zb+ZR-1 of the item's column tile, halos
+// included -- into the ring of S slots, in order.  A slot is reused once the
+// consumer warps have released its previous plane (empty barrier); a TMA copy
+// signals `full` by bytes, the plain-load path by 32 arrivals.  Every wait is
 // bounded: on expiry the error word is set and staging stops.  Before
-// returning, the last use of every slot must have landed.
-template <typename TS, int R, int S, typename C>
+// returning, the last use of every slot must have landed.  Column tiles are
+// C::TX wide; tile row ty starts at grid row ty*YSTRIDE - YOFF (the kernels
+// with fused steps overlap their tiles by YOFF rows on each side).
+template <typename TS, int R, int S, typename C, int ZR = R, int YSTRIDE = C::TY,
+          int YOFF = 0>
 __device__ __forceinline__ void produce_planes(const CUtensorMap& map, const TS* __restrict__ src,
                                                const Work3D& w, TS* slots, uint64_t* full,
                                                uint64_t* empty, int lane) {
   using TA = typename C::TA;
-  constexpr int XW = C::XW, HX = C::HX, RYM = C::RYM, TY = C::TY;
+  constexpr int XW = C::XW, HX = C::HX, RYM = C::RYM;
   const int64_t nx = w.nx, ny = w.ny, nz = w.nz, nxy = nx * ny;
   uint32_t n = 0;  // planes issued so far (ring position)
   bool ok = true;
   for (int64_t it = blockIdx.x; ok && it < w.items; it += gridDim.x) {
     const Seg3D sg = item_seg(it, w);
     const int tx = (int)(sg.tile % w.ntx), ty = (int)(sg.tile / w.ntx);
-    const int gx = tx * C::TX - HX, gy = ty * TY - RYM;
-    for (int64_t p = sg.za - R; p < sg.zb + R; ++p, ++n) {
+    const int gx = tx * C::TX - HX, gy = ty * YSTRIDE - YOFF - RYM;
+    for (int64_t p = sg.za - ZR; p < sg.zb + ZR; ++p, ++n) {
       const int s = n % S;
       const unsigned use = n / S;
       if (use > 0 && !mbar_wait(&empty[s], (use - 1) & 1, w.wait_ns)) {

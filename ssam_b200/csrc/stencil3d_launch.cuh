@@ -10,7 +10,7 @@
 #include <map>
 #include <mutex>
 
-#include "stencil3d_zreg.cuh"
+#include "stencil3d_t2.cuh"
 
 namespace ssam {
 
@@ -44,17 +44,39 @@ struct Launch3D {
   bool prepare_only;  // resolve attributes/occupancy/symbols, launch nothing
 };
 
+// Dynamic shared memory of a 3D CTA and the rows a column tile stores: those
+// of Stencil3DCfg for single-step launches, of Stencil3DT2Cfg (tiles that
+// overlap by 2R rows) for two-step ones.
+template <int T_, typename TS, int SH, int R, int PY, int NW, int S, int V_>
+struct Geom3D {
+  static constexpr int SMEM = Stencil3DCfg<TS, SH, R, PY, NW, S, V_>::SMEM;
+  static constexpr int TYS = Stencil3DCfg<TS, SH, R, PY, NW, S, V_>::TY;
+};
+template <typename TS, int SH, int R, int PY, int NW, int S, int V_>
+struct Geom3D<2, TS, SH, R, PY, NW, S, V_> {
+  static constexpr int SMEM = Stencil3DT2Cfg<TS, SH, R, PY, NW, S, V_>::SMEM;
+  static constexpr int TYS = Stencil3DT2Cfg<TS, SH, R, PY, NW, S, V_>::OY;
+};
+
 // ZREG: the kernel of stencil3d_zreg.cuh (own cells in a register ring
-// along z) instead of stencil3d_kernel.
+// along z) instead of stencil3d_kernel.  T_ = 2: the kernel of
+// stencil3d_t2.cuh, two time steps per launch (no right-hand side).
 template <typename TS, int SH, int R, int PY, int NW, int S, bool RHS = false,
-          bool ZREG = false, int V_ = 4>
+          bool ZREG = false, int V_ = 4, int T_ = 1>
 int launch_3d(const Launch3D& a) {
+  static_assert(T_ == 1 || (T_ == 2 && !RHS && !ZREG), "fused launches: two steps, no rhs");
   using C = Stencil3DCfg<TS, SH, R, PY, NW, S, V_>;
   using TA = typename C::TA;
   auto kern = [] {
-    if constexpr (ZREG) return &stencil3d_zreg_kernel<TS, SH, R, PY, NW, S, RHS, V_>;
+    if constexpr (T_ == 2) return &stencil3d_t2_kernel<TS, SH, R, PY, NW, S, V_>;
+    else if constexpr (ZREG) return &stencil3d_zreg_kernel<TS, SH, R, PY, NW, S, RHS, V_>;
     else return &stencil3d_kernel<TS, SH, R, PY, NW, S, RHS, V_>;
   }();
+  // dynamic shared memory, rows stored per column tile, input planes staged
+  // beyond each end of a z chunk
+  constexpr int SMEM = Geom3D<T_, TS, SH, R, PY, NW, S, V_>::SMEM;
+  constexpr int TYS = Geom3D<T_, TS, SH, R, PY, NW, S, V_>::TYS;
+  constexpr int ZR = T_ * R;
   if ((a.rhs != nullptr) != RHS)
     return fail(SSAM_ERR_INVALID, "3D kernel instance does not match the right-hand side");
   static std::mutex mu;
@@ -67,10 +89,10 @@ int launch_3d(const Launch3D& a) {
     auto it = ctas_per_sm.find(dev);
     if (it == ctas_per_sm.end()) {
       SSAM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         C::SMEM));
+                                         SMEM));
       int b = 0;
       SSAM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, C::THREADS,
-                                                                  C::SMEM));
+                                                                  SMEM));
       if (b < 1) return fail(SSAM_ERR_UNSUPPORTED, "3D kernel does not fit on an SM");
       it = ctas_per_sm.emplace(dev, b).first;
     }
@@ -87,8 +109,9 @@ int launch_3d(const Launch3D& a) {
   w.rhs = a.rhs;
   w.rhs_scale = a.rhs_scale;
   w.ntx = (int)((a.nx + C::TX - 1) / C::TX);
-  w.nty = (int)((a.ny + C::TY - 1) / C::TY);
-  // z chunk: minimise (rounds of items) x (chunk + 2R prologue planes)
+  w.nty = (int)((a.ny + TYS - 1) / TYS);
+  // z chunk: minimise (rounds of items) x (chunk + the 2*T*R planes staged
+  // beyond its ends; a fused launch also forms 2R extra level-1 planes)
   const int64_t grid_max = (int64_t)sms * bps;
   const int64_t ntiles = (int64_t)w.ntx * w.nty;
   int64_t best = -1;
@@ -96,7 +119,7 @@ int launch_3d(const Launch3D& a) {
     if (zc > 2 * a.nz && zc > 8) break;
     const int64_t items = ntiles * ((a.nz + zc - 1) / zc) * a.nb;
     const int64_t rounds = (items + grid_max - 1) / grid_max;
-    const int64_t cost = rounds * (std::min<int64_t>(zc, a.nz) + 2 * R);
+    const int64_t cost = rounds * (T_ * std::min<int64_t>(zc, a.nz) + 2 * ZR);
     if (best < 0 || cost < best) {
       best = cost;
       w.zc = zc;
@@ -129,8 +152,8 @@ int launch_3d(const Launch3D& a) {
   }
   CoefBlock<TA, C::NC> cf;
   for (int k = 0; k < C::NC; ++k) cf.c[k] = (TA)a.coef[k];
-  kern<<<(unsigned)grid, C::THREADS, C::SMEM, a.stream>>>(map, (const TS*)a.src, (TS*)a.dst,
-                                                          w, cf);
+  kern<<<(unsigned)grid, C::THREADS, SMEM, a.stream>>>(map, (const TS*)a.src, (TS*)a.dst, w,
+                                                       cf);
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   cudaStreamIsCapturing(a.stream, &cap);
   if (cap == cudaStreamCaptureStatusNone) count_launch();  // graphs count at replay
@@ -142,27 +165,29 @@ using LaunchFn3D = int (*)(const Launch3D&);
 
 // One compiled configuration of a 3D stencil: rows per consumer warp (PY),
 // consumer warps per CTA (NW; the column tile is 32*V x NW*PY), ring slots
-// (S planes of the tile in shared memory), the kernel variant and the
-// columns a thread (V).  `dflt` marks the configuration
-// used when nothing was measured for the grid's size class.
+// (S planes of the tile in shared memory), the kernel variant, the columns a
+// thread (V) and the time steps one launch applies (t).  `dflt` marks the
+// configuration used when nothing was measured for the grid's size class.
 struct Cand3D {
   LaunchFn3D fn;
   int py, nw, s;
   int zreg;  // 1: own cells in a register ring along z (stencil3d_zreg.cuh)
   int v;     // columns a thread (the tile is 32*v columns)
   bool dflt;
+  int t;     // time steps per launch (2: stencil3d_t2.cuh)
 };
 
-// Adds a configuration to the table of (dtype, shape, radius, rhs term).
+// Adds a configuration to the table of (dtype, shape, radius, rhs term,
+// steps per launch).
 void register_3d(int dtype, int shape, int r, bool rhs, const Cand3D& c);
 
 template <typename TS, int SH, int R, int PY, int NW, int S, bool RHS, bool DEFAULT,
-          bool ZREG = false, int V_ = 4>
+          bool ZREG = false, int V_ = 4, int T_ = 1>
 struct Register3D {
   Register3D() {
     register_3d(Traits<TS>::DT, SH, R, RHS,
-                Cand3D{&launch_3d<TS, SH, R, PY, NW, S, RHS, ZREG, V_>, PY, NW, S, ZREG ? 1 : 0,
-                       V_, DEFAULT});
+                Cand3D{&launch_3d<TS, SH, R, PY, NW, S, RHS, ZREG, V_, T_>, PY, NW, S,
+                       ZREG ? 1 : 0, V_, DEFAULT, T_});
   }
 };
 

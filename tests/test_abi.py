@@ -33,7 +33,7 @@ def test_library_exports_declared_symbol(name):
 
 
 def test_abi_version():
-    assert S.lib().ssam_abi_version() == 1
+    assert S.lib().ssam_abi_version() == 2
 
 
 FAKE_SRC = 0x7f0000000000
@@ -111,12 +111,15 @@ def test_autotune_3d_choices_roundtrip(tmp_path):
     q = tmp_path / "again.txt"
     S.autotune_save(str(q))
     text = q.read_text()
-    assert "choice3d 0 0 2 0 9 9 9 2 16 8 1 4" in text
-    assert "choice3d 2 0 1 1 7 7 10 4 8 6 0 8" in text
+    assert "choice3d 0 0 2 0 9 9 9 2 16 8 1 4 1" in text
+    assert "choice3d 2 0 1 1 7 7 10 4 8 6 0 8 1" in text
     assert "choice 0 2 2 2 2 0 1 13 13 32 2 4" in text
     for bad_line in ("choice3d 0 0 2 0 9 9 9 2 16 8 2 4\n",   # z flag must be 0 or 1
                      "choice3d 0 0 2 0 9 9 9 0 16 8 1 4\n",   # PY >= 1
                      "choice3d 0 0 2 0 9 9 9 2 16 8 1 0\n",   # V >= 1
+                     "choice3d 0 0 2 0 9 9 9 2 16 8 0 4 3\n",  # 1 or 2 steps a launch
+                     "depth3d 0 0 1 9 9 9 0\n",               # depth 1 or 2
+                     "depth3d 0 0 1 9 9\n",
                      "choice3d 0 0 2 0 9 9\n"):
         bad = tmp_path / "bad3d.txt"
         bad.write_text(bad_line)
@@ -127,7 +130,19 @@ def test_autotune_3d_choices_roundtrip(tmp_path):
     old.write_text("choice3d 1 1 1 0 8 8 8 4 4 5 0\n")
     S.autotune_load(str(old))
     S.autotune_save(str(q))
-    assert "choice3d 1 1 1 0 8 8 8 4 4 5 0 4" in q.read_text()
+    assert "choice3d 1 1 1 0 8 8 8 4 4 5 0 4 1" in q.read_text()
+    # two-step configurations (last field t = 2) and the temporal depth of a
+    # size class are kept apart from the single-step choice of that class
+    two = tmp_path / "two3d.txt"
+    two.write_text("choice3d 0 0 1 0 9 9 9 4 8 6 0 4 2\n"
+                   "choice3d 0 0 1 0 9 9 9 2 8 8 1 8\n"
+                   "depth3d 0 0 1 9 9 9 2\n")
+    S.autotune_load(str(two))
+    S.autotune_save(str(q))
+    text = q.read_text()
+    assert "choice3d 0 0 1 0 9 9 9 4 8 6 0 4 2" in text
+    assert "choice3d 0 0 1 0 9 9 9 2 8 8 1 8 1" in text
+    assert "depth3d 0 0 1 9 9 9 2" in text
     S.autotune_clear()
     S.autotune_save(str(q))
-    assert "choice3d" not in q.read_text()
+    assert "choice3d" not in q.read_text() and "depth3d" not in q.read_text()

@@ -6,7 +6,7 @@ from collections import Counter
 
 import pytest
 
-from ssam_b200.build import instances, instances_3d, stream_instances
+from ssam_b200.build import instances, instances_3d, instances_3d_t2, stream_instances
 
 ES = {"f32": 4, "f64": 8, "bf16": 2, "f16": 2}
 SMEM_PER_CTA = 227 * 1024
@@ -82,6 +82,50 @@ def test_3d_slot_layout(inst):
             right = row * bw + col_off(31) + v + h
             assert row * bw <= left < (row + 1) * bw
             assert (nbox - 1) * boxs + row * bw <= right < (nbox - 1) * boxs + (row + 1) * bw
+
+
+def smem_3d_t2(dt, shape, r, py, nw, s, v):
+    """Dynamic shared memory of a two-step 3D CTA (Stencil3DT2Cfg::SMEM): the
+    input ring of the single-step layout plus D slots of the level-1 halo
+    rows (2R rows of 32*V elements per consumer warp, rounded to 128 bytes),
+    D = R + L + RH + 1 with L = RH = 1 for the 19-point operator, 0 for stars;
+    plus a second 128 bytes of slack."""
+    es = ES[dt]
+    rh = 1 if shape == 1 else 0
+    lag = max(0, rh + 1 - r)
+    d = r + lag + rh + 1
+    hb = (d * nw * 2 * r * 32 * v * es + 127) // 128 * 128
+    return smem_3d(dt, shape, r, py, nw, s, v) + hb + 128
+
+
+@pytest.mark.parametrize("inst", instances_3d_t2(), ids=lambda c: "-".join(map(str, c)))
+def test_3d_two_step_configuration_limits(inst):
+    """The static limits of stencil3d_t2.cuh hold for every compiled two-step
+    configuration: it fits one SM's shared memory, one x-halo value a lane
+    (2R columns x (PY + 2*EY) rows x 2 sides <= 32), 2R staged halo columns,
+    PY >= R, a ring of 2R+2 slots, a tile taller than its 2R rows of overlap,
+    and no more than 8 warps a CTA unless the registers allow it."""
+    dt, shape, r, py, nw, s, v, dflt = inst
+    es = ES[dt]
+    ey = 1 if shape == 1 else 0
+    assert smem_3d_t2(dt, shape, r, py, nw, s, v) <= SMEM_PER_CTA
+    assert 2 * r * (py + 2 * ey) <= 32
+    assert 2 * r <= 16 // es
+    assert py >= r and s >= 2 * r + 2 and nw * py > 2 * r
+    assert nw + 1 <= 9  # one CTA an SM: 168 registers a thread at 9 warps
+
+
+def test_3d_two_step_groups():
+    """One default per (dtype, shape, radius) group of two-step kernels, and
+    every group has a single-step table beside it (odd step counts)."""
+    groups = Counter((dt, shape, r) for (dt, shape, r, *_rest, dflt) in instances_3d_t2() if dflt)
+    every = {(dt, shape, r) for (dt, shape, r, *_rest) in instances_3d_t2()}
+    assert set(groups) == every and all(v == 1 for v in groups.values())
+    single = {(dt, shape, r) for (dt, shape, r, _, _, _, rhs, _, _, _) in instances_3d() if not rhs}
+    assert every <= single
+    for dt in ("f32", "bf16"):
+        for shape, r in ((0, 1), (0, 2), (1, 1)):
+            assert (dt, shape, r) in every
 
 
 def test_3d_groups_have_exactly_one_default():

@@ -16,7 +16,7 @@ import torch
 
 import oracle
 import ssam_b200 as S
-from ssam_b200.build import instances_3d
+from ssam_b200.build import instances_3d, instances_3d_t2
 from ssam_b200.workloads import gaussian_rhs
 from ssam_cases import taps_j3d13pt, taps_j3d7pt, uniform
 from test_stencil3d_gpu import band_close, cube_from_taps, magnitude, oracle_steps, poisson_cube
@@ -143,9 +143,12 @@ def test_autotune_stencil3d_then_parity(cuda, tmp_path, shape, r):
     S.autotune_clear()
     try:
         rep = S.autotune_stencil3d(t, cube, r, sh, boundary="copy")
+        # every single-step and every two-step configuration is timed
         assert rep["candidates"] == sum(1 for c in stencil_cases()
-                                        if c[0] == "f32" and c[1] == shape and c[2] == r)
+                                        if c[0] == "f32" and c[1] == shape and c[2] == r) + \
+            sum(1 for c in instances_3d_t2() if c[:3] == ("f32", shape, r))
         assert rep["ms_per_step"] > 0 and rep["consumer_warps"] >= 1
+        assert rep["fused_steps"] in (1, 2)
         got = S.stencil3d(t, cube, r, sh, steps=3, boundary="copy").cpu().numpy()
         S.device_status()
         # the choice survives a save / load round trip
