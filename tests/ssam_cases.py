@@ -64,6 +64,14 @@ def taps_j3d13pt(dtype=np.float64):
 
 # seeded inputs -------------------------------------------------------------
 
+def stable_seed(*parts) -> int:
+    """A seed derived from the test's parameters that is the same in every
+    process (Python's hash() of strings is randomised per process, which
+    would make a failing case impossible to replay)."""
+    import zlib
+    return zlib.crc32(repr(parts).encode()) & 0x7FFFFFFF
+
+
 def rng(seed: int) -> np.random.Generator:
     return np.random.Generator(np.random.PCG64(seed))
 

@@ -20,7 +20,7 @@ import torch
 import oracle
 import ssam_b200 as S
 from ssam_cases import (assert_rel_close, golden, magnitude2d, normalised, rng,
-                        star_matrix, table2d, uniform)
+                        stable_seed, star_matrix, table2d, uniform)
 
 pytestmark = pytest.mark.gpu
 
@@ -94,7 +94,7 @@ SHAPES = [(1, 1), (1, 7), (7, 1), (3, 200), (17, 33), (64, 64), (131, 257), (300
                                     ("box", 2), ("box", 3), ("box", 5)])
 @pytest.mark.parametrize("bnd", ["zero", "copy", "clamp"])
 def test_stencil_family_vs_oracle(cuda, dt, shape, kind, r, bnd):
-    seed = hash((shape, kind, r, bnd, dt.__name__)) % 2**31
+    seed = stable_seed(shape, kind, r, bnd, dt.__name__)
     src = uniform(shape, -1, 1, dt, seed)
     f = 2 * r + 1
     if kind == "star":
@@ -134,7 +134,7 @@ def test_conv_non_square_vs_oracle(cuda, fh, fw):
 def test_multistep_vs_oracle(cuda, dt, kind, r, steps, bnd):
     """Temporal blocking (steps fused in registers) and launch chaining."""
     shape = (150, 333)
-    seed = hash((kind, r, steps, bnd)) % 2**31
+    seed = stable_seed(kind, r, steps, bnd)
     src = uniform(shape, 0, 1, dt, seed)
     f = 2 * r + 1
     if kind == "star":
@@ -176,7 +176,7 @@ def test_pitched_and_unaligned_grids(cuda):
                                           ("star", 1, 4), ("box", 1, 8)])
 def test_half_storage_vs_fp64_oracle(cuda, tdt, rel, kind, r, steps):
     shape = (123, 517)
-    seed = hash((kind, r, steps)) % 2**31
+    seed = stable_seed(kind, r, steps)
     src32 = uniform(shape, 0, 1, np.float32, seed)
     t = torch.from_numpy(src32).to(tdt)
     src64 = t.double().numpy()
