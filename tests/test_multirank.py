@@ -89,39 +89,117 @@ import numpy as np, torch
 import oracle
 from ssam_b200 import shard, slab
 r = shard.init("gloo", timeout_s=30)
-H, W, radius, steps, depth = {H}, {W}, {radius}, {steps}, {depth}
+H, W, radius, steps, depth, bnd = {H}, {W}, {radius}, {steps}, {depth}, {bnd!r}
 g = np.random.Generator(np.random.PCG64(5))
 grid = g.uniform(-1, 1, size=(H, W))
 m = g.random((2 * radius + 1, 2 * radius + 1)); m /= m.sum()
 mine = shard.partition(H, r.rank, r.world)
 local = torch.from_numpy(grid[mine.start:mine.stop].copy())
 # the oracle stands in for the GPU kernel on the extended band (test only)
-compute = lambda ext, t: torch.from_numpy(oracle.conv2d(ext.numpy(), m, "zero", steps=t))
+compute = lambda ext, t: torch.from_numpy(oracle.conv2d(ext.numpy(), m, bnd, steps=t))
 out = slab.run(local, H, radius, steps, depth, compute)
-want = oracle.conv2d(grid, m, "zero", steps=steps)[mine.start:mine.stop]
+want = oracle.conv2d(grid, m, bnd, steps=steps)[mine.start:mine.stop]
 print(json.dumps({{"rank": r.rank, "maxerr": float(np.abs(out.numpy() - want).max())}}),
       flush=True)
 shard.finish()
 """
 
+ZSLAB_WORKER = r"""
+import os, sys, json
+sys.path.insert(0, {root!r})
+import numpy as np, torch
+import oracle
+from ssam_b200 import shard, slab
+r = shard.init("gloo", timeout_s=30)
+NZ, radius, steps, depth, bnd, p19 = {NZ}, {radius}, {steps}, {depth}, {bnd!r}, {p19}
+g = np.random.Generator(np.random.PCG64(9))
+grid = g.uniform(0, 1, size=(NZ, 11, 13))
+f = 2 * radius + 1
+taps = [(dz, dy, dx, g.random()) for dz in range(-radius, radius + 1)
+        for dy in range(-radius, radius + 1) for dx in range(-radius, radius + 1)
+        if (abs(dz) + abs(dy) + abs(dx) <= 2 if p19 else (dz, dy, dx).count(0) >= 2)]
+mine = shard.partition(NZ, r.rank, r.world)
+local = torch.from_numpy(grid[mine.start:mine.stop].copy())
+def steps3d(a, t):
+    for _ in range(t):
+        a = oracle.taps3d(a, taps, bnd)
+    return a
+# the oracle stands in for the GPU kernel on the extended band (test only)
+compute = lambda ext, t: torch.from_numpy(steps3d(ext.numpy(), t))
+out = slab.run(local, NZ, radius, steps, depth, compute)
+want = steps3d(grid, steps)[mine.start:mine.stop]
+print(json.dumps({{"rank": r.rank, "maxerr": float(np.abs(out.numpy() - want).max())}}),
+      flush=True)
+shard.finish()
+"""
 
-@pytest.mark.parametrize("world,H,radius,steps,depth", [(2, 40, 1, 5, 2), (3, 31, 2, 4, 4),
-                                                         (2, 12, 2, 3, 1)])
-def test_row_slabs_with_halo_exchange_match_the_whole_grid(world, H, radius, steps, depth):
-    """Row slabs over gloo ranks, halos of radius * depth rows swapped before
-    every temporal block: each rank's rows equal the same steps on the whole
-    grid (bit for bit: the same arithmetic on the same values)."""
+GUARD_WORKER = r"""
+import os, sys, json
+sys.path.insert(0, {root!r})
+import torch
+from ssam_b200 import shard, slab
+r = shard.init("gloo", timeout_s=20)
+mine = shard.partition({H}, r.rank, r.world)
+try:
+    slab.run(torch.zeros(mine.stop - mine.start, 5), {H}, {radius}, 3, {depth},
+             lambda ext, t: ext)
+    print(json.dumps({{"rank": r.rank, "raised": False}}), flush=True)
+except ValueError:
+    print(json.dumps({{"rank": r.rank, "raised": True}}), flush=True)
+shard.finish()
+"""
+
+
+def run_workers(world, code_of_rank, timeout=180):
     import json
     port = free_port()
     procs = []
     for rank in range(world):
         env = dict(os.environ, RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank),
                    MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
-        code = SLAB_WORKER.format(root=ROOT, H=H, W=23, radius=radius, steps=steps, depth=depth)
-        procs.append(subprocess.Popen([sys.executable, "-c", code], env=env,
+        procs.append(subprocess.Popen([sys.executable, "-c", code_of_rank], env=env,
                                       stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+    out = []
     for p in procs:
-        out, err = p.communicate(timeout=180)
+        o, err = p.communicate(timeout=timeout)
         assert p.returncode == 0, err
-        res = json.loads(out.strip().splitlines()[-1])
+        out.append(json.loads(o.strip().splitlines()[-1]))
+    return out
+
+
+@pytest.mark.parametrize("world,H,radius,steps,depth,bnd",
+                         [(2, 40, 1, 5, 2, "zero"), (3, 31, 2, 4, 4, "zero"),
+                          (2, 12, 2, 3, 1, "zero"), (2, 40, 1, 5, 2, "copy"),
+                          (3, 31, 2, 4, 4, "copy")])
+def test_row_slabs_with_halo_exchange_match_the_whole_grid(world, H, radius, steps, depth, bnd):
+    """Row slabs over gloo ranks, halos of radius * depth rows swapped before
+    every temporal block: each rank's rows equal the same steps on the whole
+    grid (bit for bit: the same arithmetic on the same values), under the
+    ZERO and the COPY boundary."""
+    code = SLAB_WORKER.format(root=ROOT, H=H, W=23, radius=radius, steps=steps, depth=depth,
+                              bnd=bnd)
+    for res in run_workers(world, code):
         assert res["maxerr"] == 0.0, res
+
+
+@pytest.mark.parametrize("world,NZ,radius,steps,depth,bnd,p19",
+                         [(2, 20, 1, 5, 2, "zero", False), (3, 25, 2, 4, 2, "copy", False),
+                          (2, 18, 1, 4, 2, "copy", True), (3, 16, 1, 3, 1, "zero", True)])
+def test_z_slabs_of_a_3d_grid_match_the_whole_grid(world, NZ, radius, steps, depth, bnd, p19):
+    """z-slabs of one 3D grid (star r = 1, 2 and the 19-point pattern), halos
+    of radius * depth planes swapped before every temporal block: each rank's
+    planes equal the steps on the whole grid bit for bit, ZERO and COPY."""
+    code = ZSLAB_WORKER.format(root=ROOT, NZ=NZ, radius=radius, steps=steps, depth=depth,
+                               bnd=bnd, p19=p19)
+    for res in run_workers(world, code):
+        assert res["maxerr"] == 0.0, res
+
+
+def test_too_thin_bands_fail_on_every_rank():
+    """10 rows over 3 ranks give bands of 4, 3 and 3; a halo of 4 rows is
+    thicker than the thinnest band, so every rank (the one owning 4 rows
+    too) raises before any exchange instead of one of them waiting for
+    peers that gave up."""
+    code = GUARD_WORKER.format(root=ROOT, H=10, radius=2, depth=2)
+    res = run_workers(3, code, timeout=60)
+    assert all(r["raised"] for r in res), res
