@@ -136,6 +136,12 @@ int check_grid2d(const void* src, const void* dst, int64_t w, int64_t h,
     return fail(SSAM_ERR_INVALID, "width/height above 2^31");
   if (!valid_dtype(dtype)) return fail(SSAM_ERR_INVALID, "unknown dtype");
   if (!valid_boundary(boundary)) return fail(SSAM_ERR_INVALID, "unknown boundary");
+  // the grid's byte extent must be representable (pitch is otherwise unbounded)
+  uint64_t cells = 0, bytes = 0;
+  if (__builtin_mul_overflow((uint64_t)pitch, (uint64_t)h, &cells) ||
+      __builtin_mul_overflow(cells, (uint64_t)dtype_size(dtype), &bytes) ||
+      bytes > (uint64_t(1) << 62))
+    return fail(SSAM_ERR_INVALID, "pitch * height * element size overflows");
   if (grids_overlap(src, dst, w, h, pitch, dtype_size(dtype)))
     return fail(SSAM_ERR_INVALID, "src and dst overlap (updates are out of place)");
   return SSAM_OK;

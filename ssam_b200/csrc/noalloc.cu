@@ -16,9 +16,14 @@
 //    until the process exits; grids larger than it are rejected.
 //  * Host code cannot use the array's name as a device address (in host code
 //    the symbol is a host-side stand-in).  Its device address is looked up
-//    with cudaGetSymbolAddress once per device, with that device current, the
-//    first time this entry point runs on it; that first call should come
-//    before any stream capture.
+//    with cudaGetSymbolAddress, with the device current, on every call made
+//    outside stream capture (so a cudaDeviceReset, which unloads the module,
+//    never leaves a stale address behind); a call made while the stream is
+//    being captured uses the address found by the last uncaptured call on
+//    that device, so the first call on a device should come before any
+//    capture.  Under lazy module loading (the CUDA 12 default) the array is
+//    reserved when the library's module is first loaded on a device, which
+//    can be this first call: it can then fail with an out-of-memory error.
 //  * Every call shares the one array, and it keeps the last call's contents.
 //    Nothing in it has to start at zero: each launch writes every cell of the
 //    grid it produces before the next launch reads it.  Calls that overlap on
@@ -35,8 +40,9 @@ namespace ssam {
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[SSAM_NOALLOC_SCRATCH_BYTES];
 
-// Device address of g_noalloc_scratch on the current device.
-static int noalloc_scratch(void** out) {
+// Device address of g_noalloc_scratch on the current device: looked up
+// afresh unless `capturing` (then the last address found on this device).
+static int noalloc_scratch(void** out, bool capturing) {
   static std::mutex mu;
   static void* addr[64] = {};
   int dev = 0;
@@ -44,7 +50,10 @@ static int noalloc_scratch(void** out) {
   if (e != cudaSuccess) return fail_cuda(e, "cudaGetDevice");
   if (dev < 0 || dev >= 64) return fail(SSAM_ERR_UNSUPPORTED, "device ordinal above 63");
   std::lock_guard<std::mutex> g(mu);
-  if (!addr[dev]) {
+  if (capturing && !addr[dev])
+    return fail(SSAM_ERR_INVALID,
+                "ssam_stencil2d_noalloc: first call on this device is under stream capture");
+  if (!capturing) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return fail_cuda(e, "cudaGetSymbolAddress(no-alloc scratch)");
@@ -95,6 +104,7 @@ extern "C" int ssam_stencil2d_noalloc(const void* src, void* dst, int64_t width,
       }
   void* scratch = nullptr;
   if (chain.size() > 1) {
+    // no overflow: check_grid2d bounded pitch * height * element size
     const size_t need = (size_t)(pitch * height) * dtype_size(dtype);
     if (need > (size_t)SSAM_NOALLOC_SCRATCH_BYTES)
       return fail(SSAM_ERR_INVALID,
@@ -102,7 +112,10 @@ extern "C" int ssam_stencil2d_noalloc(const void* src, void* dst, int64_t width,
                       " bytes of scratch; ssam_stencil2d_noalloc holds at most " +
                       std::to_string((size_t)SSAM_NOALLOC_SCRATCH_BYTES) +
                       " bytes (pitch * height * element size)");
-    st = noalloc_scratch(&scratch);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t ce = cudaStreamIsCapturing((cudaStream_t)stream, &cap);
+    if (ce != cudaSuccess) return fail_cuda(ce, "cudaStreamIsCapturing");
+    st = noalloc_scratch(&scratch, cap != cudaStreamCaptureStatusNone);
     if (st != SSAM_OK) return st;
   }
   cudaStream_t s = (cudaStream_t)stream;

@@ -13,7 +13,9 @@ import numpy as np
 import pytest
 import torch
 
+import oracle
 import ssam_b200 as S
+from ssam_cases import star_matrix
 
 pytestmark = pytest.mark.gpu
 
@@ -57,6 +59,11 @@ def test_noalloc_matches_stencil2d_on_two_calls(cuda, shape, radius, steps, boun
         # parity tests (they agree exactly in practice)
         err = (got - want).abs().max().item()
         assert err <= 1e-5 * steps, f"call {call}: max |noalloc - stencil2d| = {err}"
+        # and directly against the oracle's chain of single steps
+        m = star_matrix(coeffs, radius) if shape == S.STAR else np.array(coeffs).reshape(f, f)
+        ref = oracle.conv2d(src.cpu().numpy(), m.astype(np.float32), boundary, steps=steps)
+        err = np.abs(got.cpu().numpy() - ref).max()
+        assert err <= 1e-5 * steps, f"call {call}: max |noalloc - oracle| = {err}"
 
 
 def test_noalloc_rejects_grids_beyond_the_array(cuda):
