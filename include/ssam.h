@@ -181,9 +181,14 @@ SSAM_API int ssam_stencil2d_host(const void* h_src, void* h_dst, int64_t width,
  * library holds until exit; it calls no allocator.  A run that needs scratch
  * (more than one launch in the chain) and a grid larger than the array
  * fails with SSAM_ERR_INVALID.  The array's device address is looked up on
- * the first call on each device (make that call before any stream capture).
- * All calls share the array: calls that overlap on the GPU race, so callers
- * serialise them.
+ * every call made outside stream capture (a cudaDeviceReset in between is
+ * harmless); a call under capture reuses the last address found on that
+ * device, so the first call on each device must come before any capture
+ * (under capture it fails with SSAM_ERR_INVALID otherwise).  With lazy module
+ * loading (the CUDA 12 default) the array is reserved when the library's
+ * module first loads on a device -- possibly during this first call, which
+ * can then fail with SSAM_ERR_CUDA (out of memory).  All calls share the
+ * array: calls that overlap on the GPU race, so callers serialise them.
  */
 SSAM_API int ssam_stencil2d_noalloc(const void* src, void* dst, int64_t width,
                                     int64_t height, int64_t pitch, int dtype, int shape,
@@ -232,6 +237,19 @@ typedef enum ssam_batch_mode {
 SSAM_API int ssam_stencil2d_batched(const ssam_grid2d* grids, int ngrids, int dtype,
                                     int shape, int radius, const double* coeffs, int steps,
                                     int boundary, int mode, void* stream);
+
+/*
+ * Test hook for the bounded-wait error path; no counterpart in the reference.
+ * Every grid-wide barrier of later persistent ssam_stencil2d_batched launches
+ * waits for `extra_arrivals` more CTAs than the launch has (arrivals that
+ * never come when > 0), and gives up after `wait_ns` nanoseconds (0 = the
+ * normal 2 s).  A barrier that gives up records code 4 in the device error
+ * word and its CTA returns (nothing asynchronous is in flight there), so the
+ * context stays usable: ssam_device_status then reports SSAM_ERR_TIMEOUT.
+ * ssam_debug_batched_barrier(0, 0) restores normal operation.  Process-wide;
+ * not for production use.
+ */
+SSAM_API int ssam_debug_batched_barrier(unsigned extra_arrivals, unsigned long long wait_ns);
 
 /* -------------------------------------------------------------- autotuner */
 

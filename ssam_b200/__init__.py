@@ -83,6 +83,10 @@ def _declare(lib):
     lib.ssam_device_status.restype = _int
     lib.ssam_device_status.argtypes = [_vp]
     lib.ssam_trim_scratch.restype = _int
+    lib.ssam_debug_batched_barrier.restype = _int
+    lib.ssam_debug_batched_barrier.argtypes = [ctypes.c_uint, ctypes.c_ulonglong]
+    lib.ssam_stencil2d_noalloc.restype = _int
+    lib.ssam_stencil2d_noalloc.argtypes = lib.ssam_stencil2d.argtypes
     lib.ssam_stencil2d_batched.restype = _int
     lib.ssam_stencil2d_batched.argtypes = [ctypes.POINTER(Grid2D), _int, _int, _int, _int, _dp,
                                            _int, _int, _int, _vp]

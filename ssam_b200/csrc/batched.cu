@@ -13,6 +13,7 @@
 // The barrier is a monotonically increasing counter in device memory; the
 // wait is bounded by %globaltimer and records an error code on expiry (read
 // with ssam_device_status), so a lost CTA cannot hang the GPU.
+#include <atomic>
 #include <string.h>
 
 #include <algorithm>
@@ -57,7 +58,13 @@ struct BatchWork {
   unsigned* barrier;       // zeroed before the launch
   int* err;
   unsigned long long wait_ns;
+  unsigned barrier_extra;  // arrivals a phase waits for beyond the grid's own (0)
 };
+
+// Test hook (ssam_debug_batched_barrier): arrivals every grid barrier waits
+// for beyond the CTAs of the grid, and its time limit (0 = the default).
+static std::atomic<unsigned> g_dbg_extra{0};
+static std::atomic<unsigned long long> g_dbg_wait_ns{0};
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
   unsigned v;
@@ -79,7 +86,7 @@ __device__ bool batch_barrier(const BatchWork& w, unsigned k) {
     ok = 1;
     __threadfence();
     atomicAdd(w.barrier, 1u);
-    const unsigned target = (k + 1) * gridDim.x;
+    const unsigned target = (k + 1) * (gridDim.x + w.barrier_extra);
     const uint64_t t0 = gclock();
     while (ld_acquire(w.barrier) < target) {
       if (gclock() - t0 > w.wait_ns) {
@@ -207,6 +214,8 @@ static int launch_batched(BatchLaunch& a) {
   w.bnd = a.bnd;
   w.barrier = (unsigned*)((char*)meta + gbytes + 128);
   w.wait_ns = 2000ull * 1000ull * 1000ull;  // 2 s; a healthy phase takes microseconds
+  w.barrier_extra = g_dbg_extra.load();
+  if (g_dbg_wait_ns.load() != 0) w.wait_ns = g_dbg_wait_ns.load();
   st = device_error_word(&w.err);
   if (st != SSAM_OK) {
     scratch_free(meta, a.stream);
@@ -295,6 +304,17 @@ static int stream_width(int dtype) { return dtype == SSAM_BF16 || dtype == SSAM_
 }  // namespace ssam
 
 using namespace ssam;
+
+extern "C" int ssam_debug_batched_barrier(unsigned extra_arrivals,
+                                          unsigned long long wait_ns) {
+  if (extra_arrivals > 1024)
+    return fail(SSAM_ERR_INVALID, "extra_arrivals above 1024");
+  if (wait_ns > 60ull * 1000ull * 1000ull * 1000ull)
+    return fail(SSAM_ERR_INVALID, "wait_ns above 60 s");
+  g_dbg_extra.store(extra_arrivals);
+  g_dbg_wait_ns.store(wait_ns);
+  return SSAM_OK;
+}
 
 extern "C" int ssam_stencil2d_batched(const ssam_grid2d* grids, int ngrids, int dtype,
                                       int shape, int radius, const double* coeffs, int steps,

@@ -53,10 +53,29 @@ def _st2d(**kw):
     dict(src=0), dict(dst=0), dict(w=0), dict(h=-1), dict(pitch=10), dict(dtype=9),
     dict(shape=7), dict(r=0), dict(r=7), dict(shape=S.BOX, r=11), dict(coeffs=None),
     dict(steps=0), dict(bnd=5), dict(bnd=1, steps=2), dict(dst=FAKE_SRC + 128),
+    dict(pitch=1 << 62), dict(pitch=(1 << 61) + 1, h=5),  # pitch * height * 4 overflows
 ])
 def test_stencil2d_rejects_bad_arguments(kw):
     assert _st2d(**kw) == S.ERR_INVALID
     assert S.lib().ssam_last_error().decode()
+
+
+def test_noalloc_rejects_overflowing_pitch():
+    """A pitch whose pitch * height * element size wraps around 64 bits is
+    rejected before the no-allocation entry compares it with its array (it
+    would otherwise pass the size check and write outside the array)."""
+    lib = S.lib()
+    fn = lib.ssam_stencil2d_noalloc
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
+                   ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                   ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int,
+                   ctypes.c_void_p]
+    c = (ctypes.c_double * 9)(*([0.1] * 9))
+    pitch = (1 << 62) + 16  # * 64 rows * 4 bytes wraps to a small number
+    st = fn(FAKE_SRC, FAKE_DST, 64, 64, pitch, S.F32, S.BOX, 1, c, 4, 0, None)
+    assert st == S.ERR_INVALID
+    assert "overflow" in lib.ssam_last_error().decode()
 
 
 @pytest.mark.parametrize("fw,fh", [(0, 3), (3, 0), (29, 3), (3, 29)])
@@ -146,3 +165,11 @@ def test_autotune_3d_choices_roundtrip(tmp_path):
     S.autotune_clear()
     S.autotune_save(str(q))
     assert "choice3d" not in q.read_text() and "depth3d" not in q.read_text()
+
+
+def test_debug_hook_rejects_out_of_range_settings():
+    """The bounded-wait test hook validates its settings (no GPU)."""
+    lib = S.lib()
+    assert lib.ssam_debug_batched_barrier(5000, 0) == S.ERR_INVALID
+    assert lib.ssam_debug_batched_barrier(0, 10**12) == S.ERR_INVALID
+    assert lib.ssam_debug_batched_barrier(0, 0) == S.OK

@@ -7,7 +7,7 @@ import torch
 
 import oracle
 import ssam_b200 as S
-from ssam_cases import assert_rel_close, magnitude2d, normalised, rng, star_matrix
+from ssam_cases import stable_seed, assert_rel_close, magnitude2d, normalised, rng, star_matrix
 
 pytestmark = pytest.mark.gpu
 
@@ -23,7 +23,7 @@ def _grids(n, lo, hi, seed, dt=np.float32):
 @pytest.mark.parametrize("steps", [1, 3, 7, 50])
 @pytest.mark.parametrize("bnd", ["zero", "copy"])
 def test_batched_vs_oracle_and_per_grid(cuda, kind, r, steps, bnd):
-    hosts = _grids(12, 9, 300, hash((kind, r, steps)) % 2**31)
+    hosts = _grids(12, 9, 300, stable_seed(kind, r, steps))
     if kind == "star":
         c = normalised((4 * r + 1,), r)
         m = star_matrix(c, r)
@@ -98,7 +98,7 @@ def test_batched_pitched_grids_stream_rows(cuda, kind, r, steps, bnd):
     row-streaming warp tiles (widths need not be a multiple of the strip's
     chunk); results equal the oracle's and, bit for bit, the per-grid
     launches', and nothing beyond each grid's width is written."""
-    hosts = _grids(14, 1, 260, hash((kind, r, steps, bnd)) % 2**31)
+    hosts = _grids(14, 1, 260, stable_seed(kind, r, steps, bnd))
     if kind == "star":
         c = normalised((4 * r + 1,), r)
         m = star_matrix(c, r)
@@ -137,3 +137,32 @@ def test_batched_pitched_other_dtypes_and_clamp(cuda, tdt, rel, bnd):
         want = oracle.conv2d(x, m, bnd, steps=steps)
         scale = np.maximum(np.abs(want), magnitude2d(x, m, bnd, steps))
         assert_rel_close(a.double().cpu().numpy(), want, scale, rel * steps, f"{tdt} {bnd}")
+
+
+def test_grid_barrier_that_gives_up_reports_a_timeout(cuda):
+    """The bounded-wait error path on the GPU, in the allowed form: a test
+    hook makes every grid barrier of the persistent launch wait for one CTA
+    more than the launch has, with a 1 ms limit.  Every CTA gives up at the
+    first barrier (no copy or MMA is in flight there), records code 4 and
+    returns; ssam_device_status reports SSAM_ERR_TIMEOUT, and with the hook
+    off the next call on the same device succeeds and matches the oracle."""
+    lib = S.lib()
+    hosts = _grids(6, 40, 200, 77)
+    srcs = [torch.from_numpy(h).to(cuda) for h in hosts]
+    coeffs = [0.2] * 5
+    assert lib.ssam_debug_batched_barrier(1, 1_000_000) == S.OK
+    try:
+        S.stencil2d_batched(srcs, coeffs, 1, S.STAR, steps=6, boundary="copy")
+        with pytest.raises(S.SsamError) as exc:
+            S.device_status()
+        assert exc.value.status == S.ERR_TIMEOUT
+        assert "code 4" in str(exc.value)
+    finally:
+        assert lib.ssam_debug_batched_barrier(0, 0) == S.OK
+    outs = S.stencil2d_batched(srcs, coeffs, 1, S.STAR, steps=6, boundary="copy")
+    S.device_status()
+    m = star_matrix(coeffs, 1).astype(np.float32)
+    for h, o in zip(hosts, outs):
+        want = oracle.conv2d(h, m, "copy", steps=6)
+        assert np.abs(o.cpu().numpy() - want).max() <= 6e-5
+
