@@ -412,11 +412,11 @@ def build_cli() -> None:
         out = os.path.join(BIN, exe)
         if (os.path.exists(out) and os.path.getmtime(out) >= os.path.getmtime(src)
                 and os.path.getmtime(out) >= os.path.getmtime(LIB)
-                and os.path.getmtime(out) >= os.path.getmtime(os.path.join(HERE, "cli",
-                                                                           "ssai_cli.h"))):
+                and all(os.path.getmtime(out) >= os.path.getmtime(os.path.join(HERE, "cli", h))
+                        for h in ("ssai_cli.h", "ref_tables.h"))):
             continue
-        cmd = [_nvcc(), "-O2", "-std=c++17", "-I", inc, src, "-o", out, "-L", HERE,
-               "-lssam_b200", "-Xlinker", "-rpath,$ORIGIN/.."]
+        cmd = [_nvcc(), "-O2", "-std=c++17", "-Xcompiler", "-fopenmp", "-I", inc, src, "-o",
+               out, "-L", HERE, "-lssam_b200", "-lgomp", "-Xlinker", "-rpath,$ORIGIN/.."]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"building {exe} failed:\n{r.stdout}\n{r.stderr}")

@@ -35,9 +35,25 @@ def test_unknown_stencil_name_is_refused():
                                  "tmp_9"])
 @pytest.mark.parametrize("dtype", ["float", "double"])
 def test_2dstencil_names(cuda, pts, dtype):
+    """Every stencil name runs the reference test's computation (its table,
+    input recipe and step count) and passes the band check against the
+    reference's Convolution applied on the host, printing its "verify dif"."""
     r = run("ssai-2dstencil", 1000, pts, dtype)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert "max relative error" in r.stdout
+    assert "max relative error" in r.stdout and "verify dif =" in r.stdout
+    if pts.startswith("tmp"):
+        assert f"Iterative={5 if pts == 'tmp_5' else 3}" in r.stdout
+
+
+@pytest.mark.gpu
+def test_2dstencil_runs_repeat_with_a_fixed_seed(cuda):
+    """The reference's rand()-drawn inputs and taps come from srand(SSAM_SEED)
+    (default 1), so two runs print the same verify line."""
+    a = run("ssai-2dstencil", 512, "5", "float")
+    b = run("ssai-2dstencil", 512, "5", "float")
+    la = [l for l in a.stdout.splitlines() if l.startswith("verify dif")]
+    lb = [l for l in b.stdout.splitlines() if l.startswith("verify dif")]
+    assert a.returncode == 0 and la == lb
 
 
 @pytest.mark.gpu
@@ -51,11 +67,25 @@ def test_2dconv_sizes(cuda, fsize, dtype):
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["7pt", "13pt", "poisson"])
 @pytest.mark.parametrize("dtype", ["float", "double"])
-@pytest.mark.parametrize("n,it", [(64, 1), (48, 3)])
+@pytest.mark.parametrize("n,it", [(64, 1), (48, 2)])
 def test_3dstencil_names(cuda, name, dtype, n, it):
     r = run("ssai-3dstencil", name, dtype, n, it)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "RMS Error" in r.stdout
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,its", [("7pt", [2, 3, 3, 4]), ("13pt", [2]), ("poisson", [2, 3, 3])])
+def test_3dstencil_runs_the_reference_sequence(cuda, name, its):
+    """Without an IT argument the program runs the reference's sequence of
+    ITERATIVE_COUNT tests, each on a fresh rand() grid, each passing
+    checkError3D's RMS tolerance."""
+    r = run("ssai-3dstencil", name, "float", 64)
+    assert r.returncode == 0, r.stdout + r.stderr
+    got = [int(l.split("ITERATIVE_COUNT=")[1].split(":")[0]) for l in r.stdout.splitlines()
+           if "ITERATIVE_COUNT=" in l]
+    assert got == its
+    assert r.stdout.count("[Test] RMS Error") == len(its)
 
 
 @pytest.mark.gpu
