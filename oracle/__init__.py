@@ -29,11 +29,18 @@ _i64 = ctypes.c_int64
 _vp = ctypes.c_void_p
 
 
+def reference_dir() -> str:
+    """The reference checkout: $SSAM_REFERENCE_DIR, else a directory named
+    ``reference`` beside this repository's checkout."""
+    return os.environ.get("SSAM_REFERENCE_DIR",
+                          os.path.join(os.path.dirname(os.path.dirname(_HERE)), "reference"))
+
+
 def build(ref: bool | None = None) -> None:
     """Compile the restatement, and the reference golds when the reference
     tree is present (``ref=None``) or when asked (``ref=True``)."""
     targets = ["all"]
-    refdir = os.environ.get("SSAM_REFERENCE_DIR", "/root/reference")
+    refdir = reference_dir()
     if ref or (ref is None and os.path.isdir(refdir)):
         targets.append("ref")
     subprocess.run(["make", "-s", "-C", _HERE, f"REF={refdir}", *targets],

@@ -1,7 +1,8 @@
 """Generate the committed golden fixtures for the SSAM stencil path.
 
-Run in a checkout that has the reference tree (default /root/reference, or
-$SSAM_REFERENCE_DIR) and a built ``oracle/_ref`` (``make -C oracle ref``):
+Run where the reference tree is readable ($SSAM_REFERENCE_DIR, else a
+directory named ``reference`` beside this checkout) and ``oracle/_ref`` is
+built (``make -C oracle ref``):
 
     python tests/golden/make_golden.py
 
@@ -32,7 +33,7 @@ sys.path.insert(0, ROOT)
 
 import oracle  # noqa: E402
 
-REF = os.environ.get("SSAM_REFERENCE_DIR", "/root/reference")
+REF = oracle.reference_dir()
 
 # 2D tables: name -> (file, which `DataType filter` block in the file)
 TABLES_2D = {
