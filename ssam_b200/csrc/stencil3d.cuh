@@ -221,6 +221,35 @@ __device__ __forceinline__ void store_row(TS* p, const TA (&o)[V]) {
   }
 }
 
+// Boundary bookkeeping of one thread's PY x V strip for the store paths.
+// xring: the columns of this lane inside the COPY ring along x (only lanes at
+// the grid's x faces have any); fast: warp-uniform -- every lane that stores
+// has all its rows in the grid and whole vector stores, and no row of the
+// warp's strip lies in the COPY ring along y.  A fast warp stores each plane
+// without per-row checks (the x ring by a per-lane column mask), so the rare
+// edge lanes do not send their whole warp down the general path.
+struct StripEdges {
+  unsigned xring;
+  bool fast;
+};
+template <int R, int PY, int V>
+__device__ __forceinline__ StripEdges strip_edges(int64_t x0, int64_t y0, int64_t nx,
+                                                  int64_t ny, int boundary, unsigned rows_ok,
+                                                  bool vec_seg) {
+  StripEdges e;
+  e.xring = 0;
+  const bool copy = boundary == SSAM_BOUNDARY_COPY;
+  if (copy) {
+#pragma unroll
+    for (int j = 0; j < V; ++j)
+      if (x0 + j < R || x0 + j >= nx - R) e.xring |= 1u << j;
+  }
+  const bool yring = copy && (y0 < R || y0 + PY > ny - R);
+  const bool lane_ok = x0 >= nx || (vec_seg && rows_ok == (1u << PY) - 1u);
+  e.fast = __all_sync(0xffffffffu, lane_ok) && !yring;
+  return e;
+}
+
 // Work item `it` = (z chunk, column tile), chunk-major.  CTAs take items
 // it = blockIdx.x + k*gridDim.x, so at any moment the grid works on a band
 // of consecutive items -- the same z chunk of neighbouring tiles -- and the
@@ -371,6 +400,7 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
     const bool vec_seg = x0 + V <= nx && (uintptr_t)outz % AL == 0 &&
                          (nx * (int64_t)sizeof(TS)) % AL == 0 &&
                          (nxy * (int64_t)sizeof(TS)) % AL == 0;
+    const StripEdges edges = strip_edges<R, PY, V>(x0, y0, nx, ny, w.boundary, row_ok, vec_seg);
     // right-hand side rows, kept as raw 32-bit words: 2-byte types load plane
     // z+1 while plane z is computed (software pipelined across the z loop);
     // wider types load plane z at the top of its iteration (registers)
@@ -529,6 +559,26 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
       }
       // store PY rows x V columns
       const bool zring = w.boundary == SSAM_BOUNDARY_COPY && (z < R || z >= nz - R);
+      if (edges.fast && !zring) {
+#pragma unroll
+        for (int i = 0; i < PY; ++i) {
+          TA o[V];
+#pragma unroll
+          for (int j = 0; j < V; ++j) o[j] = acc[i][j];
+          if constexpr (RHS) {
+            TS fv[V];
+            memcpy(fv, rawc[i], sizeof(fv));
+#pragma unroll
+            for (int j = 0; j < V; ++j) o[j] = fma((TA)w.rhs_scale, to_acc(fv[j]), o[j]);
+          }
+          if (edges.xring) {
+#pragma unroll
+            for (int j = 0; j < V; ++j)
+              if ((edges.xring >> j) & 1u) o[j] = center[i][j];
+          }
+          if (x0 < nx) store_row<TS, V>(outz + i * nx, o);
+        }
+      } else {
       const bool any_ring = ring_xy || zring;
 #pragma unroll
       for (int i = 0; i < PY; ++i) {
@@ -558,6 +608,7 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
           for (int j = 0; j < V; ++j)
             if (x0 + j < nx) outp[j] = from_acc<TS>(o[j]);
         }
+      }
       }
       outz += nxy;
       if constexpr (RHS && PIPE) {

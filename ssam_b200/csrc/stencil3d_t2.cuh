@@ -207,10 +207,16 @@ stencil3d_t2_kernel(const __grid_constant__ CUtensorMap map, const TS* __restric
       const int trow = warp * PY + i;
       if (y >= 0 && y < ny && trow >= H && trow < TY - H && x0 < nx) row_st |= 1u << i;
     }
-    // does my strip touch the edge band where the boundary rule acts (ZERO:
-    // cells outside the grid; COPY: the ring of width R)?
-    const bool edge_xy = copy ? (x0 < R || x0 + V > nx - R || y0 < R || y0 + PY > ny - R)
-                              : (x0 + V > nx || y0 < 0 || y0 + PY > ny);
+    // where the boundary rule acts on level 1 (ZERO: cells outside the grid;
+    // COPY: the ring of width R): rows -- warp-uniform, handled cell by cell
+    // -- and columns -- a per-lane mask, non-zero only for lanes at the grid's
+    // x faces, so that those lanes do not send their warp down the per-cell
+    // path
+    const bool edge_y = copy ? (y0 < R || y0 + PY > ny - R) : (y0 < 0 || y0 + PY > ny);
+    unsigned xmask1 = 0;
+#pragma unroll
+    for (int j = 0; j < V; ++j)
+      if (copy ? (x0 + j < R || x0 + j >= nx - R) : (x0 + j >= nx)) xmask1 |= 1u << j;
     // the x-halo value's cell
     const int64_t egx = cx0 + xe, egy = y0 + ek;
     const bool e_out = egx < 0 || egx >= nx || egy < 0 || egy >= ny;
@@ -222,6 +228,10 @@ stencil3d_t2_kernel(const __grid_constant__ CUtensorMap map, const TS* __restric
                          (uintptr_t)(dst + (sg.b * nz + sg.za) * nxy + ybase * nx + x0) % AL == 0 &&
                          (nx * (int64_t)sizeof(TS)) % AL == 0 &&
                          (nxy * (int64_t)sizeof(TS)) % AL == 0;
+    // level 2's store: a lane that stores rows needs whole vector stores for
+    // the warp to take the fast path (rows not stored are skipped by row_st)
+    const StripEdges edges = strip_edges<R, PY, V>(x0, y0, nx, ny, w.boundary, (1u << PY) - 1u,
+                                                   vec_seg || row_st == 0);
 
     TA ring[RL][PY][V];  // level-1 own cells: plane q in slot (q - za + R) % RL
     TA ext[RL];          // level-1 x-halo value of this lane, same slots
@@ -349,22 +359,33 @@ stencil3d_t2_kernel(const __grid_constant__ CUtensorMap map, const TS* __restric
           __syncwarp();
           if (lane == 0) mbar_arrive(&empty[(n + (uint32_t)qi) % S]);
           // boundary rule, rounding to the storage type, into the register ring
-          const bool edge = edge_xy || (copy ? zring : zout);
+          if (edge_y || (copy ? zring : zout)) {
 #pragma unroll
-          for (int i = 0; i < PY; ++i) {
+            for (int i = 0; i < PY; ++i) {
 #pragma unroll
-            for (int j = 0; j < V; ++j) {
-              TA o = acc[i][j];
-              if (edge) {
+              for (int j = 0; j < V; ++j) {
+                TA o = acc[i][j];
                 const int64_t x = x0 + j, y = y0 + i;
                 if (copy) {
                   if (zring || y < R || y >= ny - R || x < R || x >= nx - R) o = center[i][j];
                 } else if (zout || !((row_in >> i) & 1u) || x >= nx) {
                   o = TA(0);
                 }
+                ring[u][i][j] = to_acc(from_acc<TS>(o));
               }
-              ring[u][i][j] = to_acc(from_acc<TS>(o));
             }
+          } else {
+            if (xmask1) {
+#pragma unroll
+              for (int i = 0; i < PY; ++i)
+#pragma unroll
+                for (int j = 0; j < V; ++j)
+                  if ((xmask1 >> j) & 1u) acc[i][j] = copy ? center[i][j] : TA(0);
+            }
+#pragma unroll
+            for (int i = 0; i < PY; ++i)
+#pragma unroll
+              for (int j = 0; j < V; ++j) ring[u][i][j] = to_acc(from_acc<TS>(acc[i][j]));
           }
           if (copy ? (e_ring || zring) : (e_out || zout)) ev = copy ? ec : TA(0);
           ext[u] = to_acc(from_acc<TS>(ev));
@@ -466,6 +487,20 @@ stencil3d_t2_kernel(const __grid_constant__ CUtensorMap map, const TS* __restric
           const int zc = (u + 2 * RL - R - L) % RL;  // ring slot of plane p2 (centre values)
           const bool zring2 = copy && (p2 < R || p2 >= nz - R);
           const bool ring_xy = copy && (x0 < R || x0 + V > nx - R || y0 < R || y0 + PY > ny - R);
+          TS* outz = dst + (sg.b * nz + p2) * nxy + y0 * nx + x0;
+          if (edges.fast && !zring2) {
+            // whole vector stores of the rows the tile keeps (the x ring by a
+            // per-lane column mask)
+#pragma unroll
+            for (int i = 0; i < PY; ++i) {
+              if (edges.xring) {
+#pragma unroll
+                for (int j = 0; j < V; ++j)
+                  if ((edges.xring >> j) & 1u) acc[i][j] = ring[zc][i][j];
+              }
+              if ((row_st >> i) & 1u) store_row<TS, V>(outz + i * nx, acc[i]);
+            }
+          } else {
 #pragma unroll
           for (int i = 0; i < PY; ++i) {
             if (!((row_st >> i) & 1u)) continue;
@@ -480,7 +515,7 @@ stencil3d_t2_kernel(const __grid_constant__ CUtensorMap map, const TS* __restric
                 if (zring2 || y < R || y >= ny - R || x < R || x >= nx - R) o[j] = ring[zc][i][j];
               }
             }
-            TS* outp = dst + (sg.b * nz + p2) * nxy + y * nx + x0;
+            TS* outp = outz + i * nx;
             if (vec_seg) {
               store_row<TS, V>(outp, o);
             } else {
@@ -488,6 +523,7 @@ stencil3d_t2_kernel(const __grid_constant__ CUtensorMap map, const TS* __restric
               for (int j = 0; j < V; ++j)
                 if (x0 + j < nx) outp[j] = from_acc<TS>(o[j]);
             }
+          }
           }
         }
         stop = consumer_bar_any(32 * NW, !ok);

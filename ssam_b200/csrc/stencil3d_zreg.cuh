@@ -102,6 +102,7 @@ stencil3d_zreg_kernel(const __grid_constant__ CUtensorMap map, const TS* __restr
     const bool vec_seg = x0 + V <= nx && (uintptr_t)outz % AL == 0 &&
                          (nx * (int64_t)sizeof(TS)) % AL == 0 &&
                          (nxy * (int64_t)sizeof(TS)) % AL == 0;
+    const StripEdges edges = strip_edges<R, PY, V>(x0, y0, nx, ny, w.boundary, row_ok, vec_seg);
     // right-hand side rows as raw 32-bit words (as in stencil3d_kernel)
     constexpr int RW = V * (int)sizeof(TS) / 4;
     constexpr bool PIPE = sizeof(TS) == 2;
@@ -286,8 +287,31 @@ stencil3d_zreg_kernel(const __grid_constant__ CUtensorMap map, const TS* __restr
         }
         // store PY rows x V columns
         const bool zring = w.boundary == SSAM_BOUNDARY_COPY && (z < R || z >= nz - R);
-        const bool any_ring = ring_xy || zring;
         const int zc = (u + R) % F;  // register slot of plane z (the centre values)
+        // (the 8-column 4- and 8-byte tiles measured faster without the
+        // separate fast store: 512^3 FP32 7-point 0.174 against 0.206 ms)
+        constexpr bool kFastStore = sizeof(TS) == 2 || V == 4;
+        if (kFastStore && edges.fast && !zring) {
+#pragma unroll
+          for (int i = 0; i < PY; ++i) {
+            TA o[V];
+#pragma unroll
+            for (int j = 0; j < V; ++j) o[j] = acc[i][j];
+            if constexpr (RHS) {
+              TS fv[V];
+              memcpy(fv, rawc[i], sizeof(fv));
+#pragma unroll
+              for (int j = 0; j < V; ++j) o[j] = fma((TA)w.rhs_scale, to_acc(fv[j]), o[j]);
+            }
+            if (edges.xring) {
+#pragma unroll
+              for (int j = 0; j < V; ++j)
+                if ((edges.xring >> j) & 1u) o[j] = zr[zc][i][j];
+            }
+            if (x0 < nx) store_row<TS, V>(outz + i * nx, o);
+          }
+        } else {
+        const bool any_ring = ring_xy || zring;
 #pragma unroll
         for (int i = 0; i < PY; ++i) {
           const int64_t y = y0 + i;
@@ -316,6 +340,7 @@ stencil3d_zreg_kernel(const __grid_constant__ CUtensorMap map, const TS* __restr
             for (int j = 0; j < V; ++j)
               if (x0 + j < nx) outp[j] = from_acc<TS>(o[j]);
           }
+        }
         }
         outz += nxy;
         if constexpr (RHS && PIPE) {
