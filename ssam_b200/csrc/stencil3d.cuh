@@ -35,6 +35,8 @@
 
 #include <cuda.h>
 
+#include <type_traits>
+
 #include "ssam_internal.cuh"
 
 namespace ssam {
@@ -218,6 +220,27 @@ __device__ __forceinline__ void store_row(TS* p, const TA (&o)[V]) {
   } else {
 #pragma unroll
     for (int k = 0; k < V; ++k) p[k] = from_acc<TS>(o[k]);
+  }
+}
+
+// acc[t] += c * src[t] over a thread's V columns (a tap with dx = 0).  For a
+// float accumulator the columns go in pairs through the packed two-lane FP32
+// FMA (FFMA2): each lane is rounded like a scalar fma, so the sums are the
+// same bits, with half the FMA instructions of the scalar loop.
+template <int V, typename TA>
+__device__ __forceinline__ void fma_row(TA (&acc)[V], TA c, const TA* src) {
+  if constexpr (std::is_same<TA, float>::value && V % 2 == 0) {
+    const float2 c2 = make_float2(c, c);
+#pragma unroll
+    for (int j = 0; j < V; j += 2) {
+      float2 a = make_float2(acc[j], acc[j + 1]);
+      a = __ffma2_rn(c2, make_float2(src[j], src[j + 1]), a);
+      acc[j] = a.x;
+      acc[j + 1] = a.y;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < V; ++j) acc[j] = fma(c, src[j], acc[j]);
   }
 }
 
@@ -517,6 +540,9 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
               if (!tap3<SH, R>(dz, dy, dx)) continue;
               const TA c = cf.c[((dz + R) * F + (dy + R)) * F + (dx + R)];
               const TA* src_row = d[i + dy + ry];
+              if (dx == 0) {
+                fma_row<V>(acc[i], c, src_row);
+              } else
 #pragma unroll
               for (int j = 0; j < V; ++j) {
                 const int t = j - dx;  // column that source column j feeds

@@ -305,6 +305,9 @@ stencil3d_t2_kernel(const __grid_constant__ CUtensorMap map, const TS* __restric
                   if (!tap3<SH, R>(dz, dy, dx)) continue;
                   const TA c = cf.c[((dz + R) * F + (dy + R)) * F + (dx + R)];
                   const TA* src_row = d[i + dy + ry];
+                  if (dx == 0) {
+                    fma_row<V>(acc[i], c, src_row);
+                  } else
 #pragma unroll
                   for (int j = 0; j < V; ++j) {
                     const int t = j - dx;
@@ -452,6 +455,9 @@ stencil3d_t2_kernel(const __grid_constant__ CUtensorMap map, const TS* __restric
                   if (!tap3<SH, R>(dz, dy, dx)) continue;
                   const TA c = cf.c[((dz + R) * F + (dy + R)) * F + (dx + R)];
                   const TA* src_row = d[i + dy + ry];
+                  if (dx == 0) {
+                    fma_row<V>(acc[i], c, src_row);
+                  } else
 #pragma unroll
                   for (int j = 0; j < V; ++j) {
                     const int t = j - dx;
