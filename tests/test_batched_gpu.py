@@ -58,23 +58,37 @@ def test_batched_other_dtypes(cuda, tdt):
         assert_rel_close(a.double().cpu().numpy(), want, scale, rel, str(tdt))
 
 
-def test_batched_256_uneven_grids_config4(cuda):
-    """The benchmark batch: 256 grids, sides log-uniform in [64, 2048], 5-pt,
-    50 steps; persistent == per-grid launches bit for bit, and grid 0 against
-    the oracle."""
+@pytest.mark.parametrize("kind,layout", [("star1", "dense"), ("star1", "pitched"),
+                                         ("box2", "pitched")])
+def test_batched_256_uneven_grids_config4(cuda, kind, layout):
+    """The benchmark batch: 256 grids, sides log-uniform in [64, 2048], the
+    5-point star or the 5x5 box, 50 steps, COPY; the persistent launch
+    equals the per-grid launches bit for bit, and every one of the 256 grids
+    matches the oracle (rel 1e-5 per step of sum|c||x|).  Dense rows take the
+    windowed phases, pitched rows (the bench's layout) the row-streaming
+    ones."""
     g = rng(256)
     sides = np.exp(g.uniform(np.log(64), np.log(2048), size=(256, 2))).astype(int)
-    srcs = [torch.rand(int(h), int(w), device=cuda) for h, w in sides]
-    c = [0.2] * 5
-    got = S.stencil2d_batched(srcs, c, 1, S.STAR, 50, "copy", persistent=True)
-    ref = S.stencil2d_batched(srcs, c, 1, S.STAR, 50, "copy", persistent=False)
+    hosts = [g.uniform(0, 1, size=(int(h), int(w))).astype(np.float32) for h, w in sides]
+    if kind == "star1":
+        r, shape, c = 1, S.STAR, [0.2] * 5
+        m = star_matrix(c, 1)
+    else:
+        r, shape = 2, S.BOX
+        m = normalised((5, 5), 257)
+        c = list(m.ravel())
+    srcs = [_pitched(h, cuda) if layout == "pitched" else torch.from_numpy(h).to(cuda)
+            for h in hosts]
+    got = S.stencil2d_batched(srcs, c, r, shape, 50, "copy", persistent=True)
+    ref = S.stencil2d_batched(srcs, c, r, shape, 50, "copy", persistent=False)
     S.device_status()
     for a, b in zip(got, ref):
         assert torch.equal(a, b)
-    h0 = srcs[0].cpu().numpy()
-    m = star_matrix(c, 1)
-    want = oracle.conv2d(h0, m.astype(np.float32), "copy", steps=50)
-    assert_rel_close(got[0].cpu().numpy(), want, magnitude2d(h0, m, "copy", 50), 5e-4, "g0")
+    mf = m.astype(np.float32)
+    for i, (h0, out) in enumerate(zip(hosts, got)):
+        want = oracle.conv2d(h0, mf, "copy", steps=50)
+        assert_rel_close(out.cpu().numpy(), want, magnitude2d(h0, m, "copy", 50), 5e-4,
+                         f"grid {i} ({h0.shape[0]} x {h0.shape[1]})")
 
 
 def _pitched(host, cuda, tdt=torch.float32):
