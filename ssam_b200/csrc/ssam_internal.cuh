@@ -7,8 +7,10 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <string.h>
 
 #include <string>
+#include <type_traits>
 
 #include "../../include/ssam.h"
 
@@ -88,6 +90,59 @@ template <> __device__ __forceinline__ __half from_acc<__half>(float v) {
 template <typename TS> __device__ __forceinline__ TS from_acc(double v);
 template <> __device__ __forceinline__ double from_acc<double>(double v) { return v; }
 
+// N elements of storage held as N * sizeof(TS) / 4 whole 32-bit words, to
+// accumulator values and back.  A 16-bit word pair holds the element of the
+// lower address in its low half.  Widening BF16 is exact bit placement (a
+// bf16 is the upper half of the fp32 of the same value: one shift or one mask
+// an element); narrowing rounds both halves to nearest even in one paired
+// conversion.  The values are those of the per-element conversions.
+template <typename TS, int N, typename TA>
+__device__ __forceinline__ void words_to_acc(TA* d, const uint32_t* w) {
+  if constexpr (std::is_same<TS, __nv_bfloat16>::value) {
+#pragma unroll
+    for (int k = 0; k < N / 2; ++k) {
+      d[2 * k] = __uint_as_float(w[k] << 16);
+      d[2 * k + 1] = __uint_as_float(w[k] & 0xffff0000u);
+    }
+  } else if constexpr (std::is_same<TS, __half>::value) {
+#pragma unroll
+    for (int k = 0; k < N / 2; ++k) {
+      __half2 h;
+      memcpy(&h, &w[k], 4);
+      const float2 f = __half22float2(h);
+      d[2 * k] = f.x;
+      d[2 * k + 1] = f.y;
+    }
+  } else {
+    TS e[N];
+    memcpy(e, w, sizeof(e));
+#pragma unroll
+    for (int k = 0; k < N; ++k) d[k] = to_acc(e[k]);
+  }
+}
+
+template <typename TS, int N, typename TA>
+__device__ __forceinline__ void acc_to_words(uint32_t* w, const TA* d) {
+  if constexpr (std::is_same<TS, __nv_bfloat16>::value) {
+#pragma unroll
+    for (int k = 0; k < N / 2; ++k) {
+      const __nv_bfloat162 h = __floats2bfloat162_rn(d[2 * k], d[2 * k + 1]);
+      memcpy(&w[k], &h, 4);
+    }
+  } else if constexpr (std::is_same<TS, __half>::value) {
+#pragma unroll
+    for (int k = 0; k < N / 2; ++k) {
+      const __half2 h = __floats2half2_rn(d[2 * k], d[2 * k + 1]);
+      memcpy(&w[k], &h, 4);
+    }
+  } else {
+    TS e[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) e[k] = from_acc<TS>(d[k]);
+    memcpy(w, e, sizeof(e));
+  }
+}
+
 // V consecutive elements starting at a 16-byte aligned address, as 16-byte
 // (128-bit) transactions.
 template <typename TS, int V, typename TA>
@@ -98,9 +153,8 @@ __device__ __forceinline__ void load_vec(TA (&r)[V], const TS* __restrict__ p) {
 #pragma unroll
   for (int c = 0; c < CH; ++c) {
     const uint4 u = __ldg(reinterpret_cast<const uint4*>(p) + c);
-    const TS* e = reinterpret_cast<const TS*>(&u);
-#pragma unroll
-    for (int k = 0; k < PER; ++k) r[c * PER + k] = to_acc(e[k]);
+    const uint32_t wd[4] = {u.x, u.y, u.z, u.w};
+    words_to_acc<TS, PER>(r + c * PER, wd);
   }
 }
 
@@ -110,11 +164,9 @@ __device__ __forceinline__ void store_vec(TS* __restrict__ p, const TA (&r)[V]) 
   constexpr int PER = 16 / sizeof(TS);
 #pragma unroll
   for (int c = 0; c < CH; ++c) {
-    uint4 u;
-    TS* e = reinterpret_cast<TS*>(&u);
-#pragma unroll
-    for (int k = 0; k < PER; ++k) e[k] = from_acc<TS>(r[c * PER + k]);
-    reinterpret_cast<uint4*>(p)[c] = u;
+    uint32_t wd[4];
+    acc_to_words<TS, PER>(wd, r + c * PER);
+    reinterpret_cast<uint4*>(p)[c] = make_uint4(wd[0], wd[1], wd[2], wd[3]);
   }
 }
 

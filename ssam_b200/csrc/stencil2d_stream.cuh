@@ -60,9 +60,8 @@ __device__ __forceinline__ void stream_unpack(TA (&d)[V], const uint4 (&w)[CH]) 
   constexpr int PER = 16 / sizeof(TS);
 #pragma unroll
   for (int c = 0; c < CH; ++c) {
-    const TS* e = reinterpret_cast<const TS*>(&w[c]);
-#pragma unroll
-    for (int k = 0; k < PER; ++k) d[c * PER + k] = to_acc(e[k]);
+    const uint32_t wd[4] = {w[c].x, w[c].y, w[c].z, w[c].w};
+    words_to_acc<TS, PER>(d + c * PER, wd);
   }
 }
 

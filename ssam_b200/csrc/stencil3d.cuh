@@ -191,15 +191,13 @@ __device__ __forceinline__ void load_slot_row(TA (&d)[V], const TS* p) {
 #pragma unroll
     for (int c = 0; c < B / 16; ++c) {
       const uint4 u = reinterpret_cast<const uint4*>(p)[c];
-      const TS* e = reinterpret_cast<const TS*>(&u);
-#pragma unroll
-      for (int k = 0; k < 16 / (int)sizeof(TS); ++k) d[c * (16 / sizeof(TS)) + k] = to_acc(e[k]);
+      const uint32_t wd[4] = {u.x, u.y, u.z, u.w};
+      words_to_acc<TS, 16 / (int)sizeof(TS)>(d + c * (16 / sizeof(TS)), wd);
     }
   } else if constexpr (B == 8) {
     const uint2 u = *reinterpret_cast<const uint2*>(p);
-    const TS* e = reinterpret_cast<const TS*>(&u);
-#pragma unroll
-    for (int k = 0; k < V; ++k) d[k] = to_acc(e[k]);
+    const uint32_t wd[2] = {u.x, u.y};
+    words_to_acc<TS, V>(d, wd);
   } else {
 #pragma unroll
     for (int k = 0; k < V; ++k) d[k] = to_acc(p[k]);
@@ -212,11 +210,9 @@ __device__ __forceinline__ void store_row(TS* p, const TA (&o)[V]) {
   if constexpr (B % 16 == 0) {
     store_vec<TS, V>(p, o);
   } else if constexpr (B == 8) {
-    uint2 u;
-    TS* e = reinterpret_cast<TS*>(&u);
-#pragma unroll
-    for (int k = 0; k < V; ++k) e[k] = from_acc<TS>(o[k]);
-    *reinterpret_cast<uint2*>(p) = u;
+    uint32_t wd[2];
+    acc_to_words<TS, V>(wd, o);
+    *reinterpret_cast<uint2*>(p) = make_uint2(wd[0], wd[1]);
   } else {
 #pragma unroll
     for (int k = 0; k < V; ++k) p[k] = from_acc<TS>(o[k]);
@@ -592,10 +588,10 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
 #pragma unroll
           for (int j = 0; j < V; ++j) o[j] = acc[i][j];
           if constexpr (RHS) {
-            TS fv[V];
-            memcpy(fv, rawc[i], sizeof(fv));
+            TA fv[V];
+            words_to_acc<TS, V>(fv, rawc[i]);
 #pragma unroll
-            for (int j = 0; j < V; ++j) o[j] = fma((TA)w.rhs_scale, to_acc(fv[j]), o[j]);
+            for (int j = 0; j < V; ++j) o[j] = fma((TA)w.rhs_scale, fv[j], o[j]);
           }
           if (edges.xring) {
 #pragma unroll
@@ -614,10 +610,10 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
 #pragma unroll
         for (int j = 0; j < V; ++j) o[j] = acc[i][j];
         if constexpr (RHS) {
-          TS fv[V];
-          memcpy(fv, rawc[i], sizeof(fv));
+          TA fv[V];
+          words_to_acc<TS, V>(fv, rawc[i]);
 #pragma unroll
-          for (int j = 0; j < V; ++j) o[j] = fma((TA)w.rhs_scale, to_acc(fv[j]), o[j]);
+          for (int j = 0; j < V; ++j) o[j] = fma((TA)w.rhs_scale, fv[j], o[j]);
         }
         if (any_ring) {
 #pragma unroll

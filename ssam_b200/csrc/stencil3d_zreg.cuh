@@ -301,10 +301,10 @@ stencil3d_zreg_kernel(const __grid_constant__ CUtensorMap map, const TS* __restr
 #pragma unroll
             for (int j = 0; j < V; ++j) o[j] = acc[i][j];
             if constexpr (RHS) {
-              TS fv[V];
-              memcpy(fv, rawc[i], sizeof(fv));
+              TA fv[V];
+              words_to_acc<TS, V>(fv, rawc[i]);
 #pragma unroll
-              for (int j = 0; j < V; ++j) o[j] = fma((TA)w.rhs_scale, to_acc(fv[j]), o[j]);
+              for (int j = 0; j < V; ++j) o[j] = fma((TA)w.rhs_scale, fv[j], o[j]);
             }
             if (edges.xring) {
 #pragma unroll
@@ -323,10 +323,10 @@ stencil3d_zreg_kernel(const __grid_constant__ CUtensorMap map, const TS* __restr
 #pragma unroll
           for (int j = 0; j < V; ++j) o[j] = acc[i][j];
           if constexpr (RHS) {
-            TS fv[V];
-            memcpy(fv, rawc[i], sizeof(fv));
+            TA fv[V];
+            words_to_acc<TS, V>(fv, rawc[i]);
 #pragma unroll
-            for (int j = 0; j < V; ++j) o[j] = fma((TA)w.rhs_scale, to_acc(fv[j]), o[j]);
+            for (int j = 0; j < V; ++j) o[j] = fma((TA)w.rhs_scale, fv[j], o[j]);
           }
           if (any_ring) {
 #pragma unroll
