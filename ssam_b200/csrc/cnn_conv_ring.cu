@@ -34,6 +34,7 @@
 //               add the optional addend, round to BF16, store valid voxels
 // Every wait is bounded by %globaltimer; on expiry the kernel records error
 // code 8 and winds down (drains its copies and MMAs, frees tensor memory).
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -343,6 +344,251 @@ __global__ void __launch_bounds__(kThreads, 1) conv3d_ring_kernel(ConvArgs a) {
   if (warp == 1) tc::tmem_free(tmem, 512);
 }
 
+// ---------------------------------------------------------------------------
+// Dilation 1 with the three z taps stacked on the MMA's N side.
+//
+// An input plane z feeds output planes z-1, z and z+1 (through the weights of
+// tap dz = +1, 0, -1).  Instead of 27 MMAs of N = 16 per output plane and
+// tile, every input plane gets 9 MMAs of N = 48 per tile (one per (dy, dx)
+// tap): the 48 accumulator columns of a tile are three 16-column slots, and
+// output plane zo accumulates in slot zo mod 3.  The B operand of input plane
+// z is the weight block permuted for z mod 3 (three copies in shared memory),
+// so that each slot receives its own output plane's tap.  After input plane
+// z, slot (z-1) mod 3 holds the finished output plane z-1: the epilogue reads
+// it, stores it, and zeroes the slot, which input plane z+1 then starts as
+// output plane z+2.  Each output plane still sums its taps in the order of
+// the 27-MMA kernel (dz = -1, 0, +1, each over the 9 (dy, dx) taps).
+//
+// Per tile one mbarrier pair hands the tile between the MMA issuer (accf:
+// input plane done) and the epilogue (acce: slot drained and zeroed), so the
+// epilogue of one tile overlaps the MMAs of the others.  The first MMA of
+// every work item does not accumulate, which clears all three slots.
+// ---------------------------------------------------------------------------
+constexpr int kZsMaxTiles = 10;  // 10 tiles x 48 columns <= 512
+constexpr int kZsWBytes = 3 * 9 * 1536;  // 3 rotations x 9 taps x (48 x 16 BF16)
+
+bool make_plan_zs(int n, Plan* p) {
+  const int xp = n + 1;
+  if (n > kMaxRow) return false;
+  for (int ty = std::min(n, 16); ty >= 1; ty /= 2) {
+    const int box_rows = ty + 2;
+    const int tiles = (ty * xp + 127) / 128;
+    if (tiles > kZsMaxTiles) continue;
+    const int tail = tiles * 128 - ty * xp + 1;
+    const int slab = ((kFrontGuard + box_rows * xp + tail) * 16 + 127) / 128 * 128;
+    const int avail = kSmemLimit - 1024 - kZsWBytes - 512;
+    const int slots = std::min(kMaxSlots, avail / (2 * slab));
+    if (slots < 3) continue;
+    const int smem = std::max(1024 + kZsWBytes + slots * 2 * slab + 512, 120 * 1024);
+    *p = Plan{ty, xp, tiles, box_rows, slab, slots, smem};
+    return true;
+  }
+  return false;
+}
+
+__global__ void __launch_bounds__(kThreads, 1) conv3d_zstack_kernel(ConvArgs a) {
+  constexpr uint32_t IDESC = tc::idesc_bf16(128, 48, 0, 0);
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  unsigned char* Ws = base;
+  unsigned char* Ring = Ws + kZsWBytes;
+  const int slot_bytes = 2 * a.slab;
+  const int S = a.slots;
+  const int T = a.tiles;
+  uint64_t* full = (uint64_t*)(Ring + S * slot_bytes);
+  uint64_t* empty = full + kMaxSlots;
+  uint64_t* accf = empty + kMaxSlots;
+  uint64_t* acce = accf + kZsMaxTiles;
+  uint64_t* drain = acce + kZsMaxTiles;
+  uint32_t* tmem_slot = (uint32_t*)(drain + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int n = a.n, xp = a.xp;
+  // weights -> B tiles: rotation rot (= input plane mod 3), tap t9 = (dy, dx);
+  // row 16k + co is output channel co of slot k, whose output plane is the
+  // one of z-1, z, z+1 that is k mod 3, so its z tap is
+  // dz = +1, 0, -1 for (rot - k) mod 3 = 1, 0, 2 (tap index dz + 1).
+  for (int idx = threadIdx.x; idx < 3 * 9 * 48 * 2; idx += kThreads) {
+    const int c = idx & 1, row = (idx >> 1) % 48, rt = (idx >> 1) / 48;
+    const int rot = rt / 9, t9 = rt % 9, k = row >> 4, co = row & 15;
+    const int m = ((rot - k) % 3 + 3) % 3;
+    const int tz = m == 0 ? 1 : (m == 1 ? 2 : 0);
+    const uint4 v = *reinterpret_cast<const uint4*>(
+        a.w + ((size_t)co * 27 + tz * 9 + t9) * a.ci_total + a.ci_off + c * 8);
+    *reinterpret_cast<uint4*>(Ws + rt * 1536 + (row >> 3) * 256 + c * 128 + (row & 7) * 16) = v;
+  }
+  for (int idx = threadIdx.x; idx < S * slot_bytes / 16; idx += kThreads)
+    reinterpret_cast<uint4*>(Ring)[idx] = make_uint4(0, 0, 0, 0);
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < S; ++i) {
+      tc::mbar_init(&full[i], 1);
+      tc::mbar_init(&empty[i], 1);
+    }
+    for (int i = 0; i < kZsMaxTiles; ++i) {
+      tc::mbar_init(&accf[i], 1);
+      tc::mbar_init(&acce[i], 128);
+    }
+    tc::mbar_init(drain, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) tc::tmem_alloc(tmem_slot, 512);
+  tc::fence_async_smem();
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  bool ok = true;
+  if (warp == 0) {
+    // ---------------------------------------------------------- producer
+    const uint32_t row_bytes = (uint32_t)n * 16;
+    const uint32_t plane_bytes = 2u * a.box_rows * row_bytes;
+    uint32_t gp = 0;
+    for (int64_t it = blockIdx.x; ok && it < a.items; it += gridDim.x) {
+      const Item m = decode(a, it);
+      for (int p = 0; p < m.len; ++p, ++gp) {
+        const int s = (int)(gp % S);
+        const uint32_t use = gp / S;
+        int good = 1;
+        if (lane == 0) {
+          if (use > 0 && !tc::mbar_wait(&empty[s], (use - 1) & 1, a.wait_ns)) good = 0;
+          if (good) mbar_expect_tx(&full[s], plane_bytes);
+        }
+        good = __shfl_sync(0xffffffffu, good, 0);
+        if (!good) {
+          ok = false;
+          break;
+        }
+        const int z = m.z0 - 1 + p;
+        const uint32_t bar = tc::smem_addr(&full[s]);
+        unsigned char* slot = Ring + s * slot_bytes;
+        for (int k = lane; k < 2 * a.box_rows; k += 32) {
+          const int h = k / a.box_rows, r = k % a.box_rows;
+          const int y = m.y0 - 1 + r;
+          const void* src = g_zero_row;
+          if (z >= 0 && z < n && y >= 0 && y < n)
+            src = a.in + h * a.half + ((((int64_t)m.b * n + z) * n + y) * n) * 8;
+          bulk_copy(tc::smem_addr(slot + h * a.slab + (kFrontGuard + r * xp + 1) * 16), src,
+                    row_bytes, bar);
+        }
+        __syncwarp();
+      }
+    }
+    if (lane == 0)
+      for (uint32_t k = gp > (uint32_t)S ? gp - S : 0; k < gp; ++k)
+        if (!tc::mbar_wait(&full[k % S], (k / S) & 1, a.wait_ns)) ok = false;
+  } else if (warp == 1) {
+    // ---------------------------------------------------------- MMA issuer
+    if (lane == 0) {
+      int toff[9];
+#pragma unroll
+      for (int t9 = 0; t9 < 9; ++t9) {
+        const int dy = t9 / 3 - 1, dx = t9 % 3 - 1;
+        toff[t9] = kFrontGuard + xp + dy * xp + dx;
+      }
+      const uint64_t abase0 = tc::smem_desc(Ring, (uint32_t)a.slab, 128);
+      const uint64_t wbase = tc::smem_desc(Ws, 128, 256);
+      uint32_t gp = 0, pc = 0;
+      bool issued = false;
+      for (int64_t it = blockIdx.x; ok && it < a.items; it += gridDim.x) {
+        const Item m = decode(a, it);
+        for (int p = 0; p < m.len; ++p, ++gp, ++pc) {
+          if (!tc::mbar_wait(&full[gp % S], (gp / S) & 1, a.wait_ns)) {
+            ok = false;
+            break;
+          }
+          const int rot = (m.z0 - 1 + p + 3) % 3;
+          const uint64_t ap = abase0 + (uint64_t)((gp % S) * (slot_bytes >> 4));
+          const uint64_t wr = wbase + (uint64_t)(rot * 9 * 96);
+          for (int t = 0; t < T; ++t) {
+            // slot (z+1) mod 3 of this tile is drained and zeroed
+            if (pc > 0 && !tc::mbar_wait(&acce[t], (pc - 1) & 1, a.wait_ns)) {
+              ok = false;
+              break;
+            }
+            tc::tc_fence_after();
+            const uint32_t d = tmem + (uint32_t)(t * 48);
+            const uint64_t at = ap + (uint64_t)(128 * t);
+#pragma unroll
+            for (int t9 = 0; t9 < 9; ++t9)
+              tc::mma_bf16(d, at + (uint64_t)toff[t9], wr + (uint64_t)(t9 * 96), IDESC,
+                           p > 0 || t9 > 0);
+            tc::mma_commit(&accf[t]);
+            issued = true;
+          }
+          if (!ok) break;
+          tc::mma_commit(&empty[gp % S]);  // the plane is read by this plane's MMAs only
+        }
+      }
+      if (issued) {
+        tc::mma_commit(drain);
+        if (!tc::mbar_wait(drain, 0, a.wait_ns)) ok = false;
+      }
+    }
+  } else {
+    // ---------------------------------------------------------- epilogue
+    const int q = warp & 3;
+    const int row = q * 32 + lane;
+    const uint32_t lanes = (uint32_t)(q * 32) << 16;
+    uint32_t pc = 0;
+    for (int64_t it = blockIdx.x; ok && it < a.items; it += gridDim.x) {
+      const Item m = decode(a, it);
+      for (int p = 0; p < m.len && ok; ++p, ++pc) {
+        const int zo = m.z0 - 2 + p;  // the output plane finished by input plane p
+        const bool store = p >= 2;    // zo in z0 .. z0 + nout - 1
+        const int k = (zo + 3) % 3;
+        const int64_t zrow = ((int64_t)m.b * n + zo) * n;
+        for (int t = 0; t < T; ++t) {
+          // (warp-uniform, for the .sync.aligned TMEM accesses below)
+          const bool got = tc::mbar_wait(&accf[t], pc & 1, a.wait_ns);
+          if (!__all_sync(0xffffffffu, got)) {
+            ok = false;
+            break;
+          }
+          tc::tc_fence_after();
+          const uint32_t col = (uint32_t)(t * 48 + k * 16);
+          if (store) {
+            float v[16];
+            tc::tmem_ld16(tmem + lanes + col, v);
+            const int pp = 128 * t + row;
+            const int r = pp / xp, x = pp % xp - 1;
+            if (r < a.ty && x >= 0 && m.y0 + r < n) {
+              const int64_t e = ((zrow + m.y0 + r) * n + x) * 8;
+#pragma unroll
+              for (int i = 0; i < 16; ++i) v[i] *= a.out_scale;
+              if (a.addend) {
+                const uint4 u0 = *reinterpret_cast<const uint4*>(a.addend + e);
+                const uint4 u1 = *reinterpret_cast<const uint4*>(a.addend + a.half + e);
+                const __nv_bfloat16* b0 = reinterpret_cast<const __nv_bfloat16*>(&u0);
+                const __nv_bfloat16* b1 = reinterpret_cast<const __nv_bfloat16*>(&u1);
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                  v[i] += __bfloat162float(b0[i]);
+                  v[8 + i] += __bfloat162float(b1[i]);
+                }
+              }
+              uint4 o[2];
+              __nv_bfloat16* ob = reinterpret_cast<__nv_bfloat16*>(o);
+#pragma unroll
+              for (int i = 0; i < 16; ++i) ob[i] = __float2bfloat16_rn(v[i]);
+              *reinterpret_cast<uint4*>(a.out + e) = o[0];
+              *reinterpret_cast<uint4*>(a.out + a.half + e) = o[1];
+            }
+          }
+          tc::tmem_zero16(tmem + lanes + col);
+          tc::tc_fence_before();
+          mbar_arrive(&acce[t]);
+        }
+      }
+    }
+  }
+  if (!ok) atomicCAS(a.err, 0, 8);
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  if (warp == 1) tc::tmem_free(tmem, 512);
+}
+
 }  // namespace
 
 // One single-source pass: out = conv(in, w[:, :, ci_off .. ci_off+15]) *
@@ -350,7 +596,13 @@ __global__ void __launch_bounds__(kThreads, 1) conv3d_ring_kernel(ConvArgs a) {
 int conv3d_ring(const void* in, const void* addend, const void* w, int ci_total, int ci_off,
                 void* out, int nb, int n, int dil, float out_scale, cudaStream_t s) {
   Plan p;
-  if (!make_plan(n, dil, &p)) return SSAM_ERR_UNSUPPORTED;
+  // dilation 1: the z-stacked kernel (9 N = 48 MMAs per input plane and
+  // tile); SSAM_CONV_RING27=1 in the environment keeps the 27-MMA kernel
+  // (to check the two against each other)
+  const char* e27 = getenv("SSAM_CONV_RING27");
+  const bool ring27 = e27 && e27[0] == '1';
+  const bool zstack = dil == 1 && !ring27 && make_plan_zs(n, &p);
+  if (!zstack && !make_plan(n, dil, &p)) return SSAM_ERR_UNSUPPORTED;
   ConvArgs a;
   a.in = (const __nv_bfloat16*)in;
   a.addend = (const __nv_bfloat16*)addend;
@@ -394,10 +646,15 @@ int conv3d_ring(const void* in, const void* addend, const void* w, int ci_total,
   if (!attr_set) {
     SSAM_CUDA_TRY(cudaFuncSetAttribute(conv3d_ring_kernel,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimit));
+    SSAM_CUDA_TRY(cudaFuncSetAttribute(conv3d_zstack_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimit));
     attr_set = true;
   }
   const int64_t grid = std::min<int64_t>(a.items, sms);
-  conv3d_ring_kernel<<<(unsigned)grid, kThreads, p.smem, s>>>(a);
+  if (zstack)
+    conv3d_zstack_kernel<<<(unsigned)grid, kThreads, p.smem, s>>>(a);
+  else
+    conv3d_ring_kernel<<<(unsigned)grid, kThreads, p.smem, s>>>(a);
   count_launch();
   SSAM_CUDA_TRY(cudaGetLastError());
   return SSAM_OK;

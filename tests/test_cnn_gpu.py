@@ -222,3 +222,23 @@ def test_cnn_training_reduces_loss_and_roundtrips(cuda, tmp_path):
     assert torch.equal(other.forward(f), u1)
     net.close()
     other.close()
+
+
+@pytest.mark.parametrize("nsrc", [1, 2])
+@pytest.mark.parametrize("n", [128, 64, 32, 16])
+def test_zstack_kernel_equals_27_mma_kernel(cuda, monkeypatch, nsrc, n):
+    """Dilation 1 runs the kernel that stacks the three z taps of an input
+    plane on the MMA's N side (9 MMAs of N = 48 per plane and tile); every
+    output still sums its taps in the 27-MMA kernel's order, so the two give
+    the same bits (SSAM_CONV_RING27=1 selects the 27-MMA kernel)."""
+    g = torch.Generator().manual_seed(7 * n + nsrc)
+    nb = 2 if n <= 64 else 1
+    xs = [torch.randn(nb, n, n, n, 16, generator=g).to(torch.bfloat16).to(cuda)
+          for _ in range(nsrc)]
+    w = (torch.randn(16, 27, 16 * nsrc, generator=g) * 0.1).to(torch.bfloat16).to(cuda)
+    args = (xs[0], w, xs[1] if nsrc == 2 else None)
+    got = S.cnn_conv3d(*args, dilation=1, scale=0.75)
+    monkeypatch.setenv("SSAM_CONV_RING27", "1")
+    want = S.cnn_conv3d(*args, dilation=1, scale=0.75)
+    S.device_status()
+    assert torch.equal(got, want)
