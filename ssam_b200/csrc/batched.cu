@@ -133,11 +133,11 @@ batched_kernel(BatchWork w, CoefBlock<typename Traits<TS>::TA, (2 * R + 1) * (2 
 // is one SEG-row segment of one warp strip of one grid; single steps only.
 // Every grid must have 16-byte aligned buffers and a pitch that is a multiple
 // of V (checked by the entry point).
-template <typename TS, int R, bool STAR, int SEG, int V>
+template <typename TS, int R, bool STAR, int SEG, int V, int DF>
 __global__ void __launch_bounds__(128)
 batched_stream_kernel(BatchWork w,
                       CoefBlock<typename Traits<TS>::TA, (2 * R + 1) * (2 * R + 1)> cf) {
-  using C = Stream2DCfg<TS, R, R, R, R, STAR, SEG, V>;
+  using C = Stream2DCfg<TS, R, R, R, R, STAR, SEG, V, DF>;
   const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
   const int64_t gw = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   for (int ph = 0; ph < w.nphases; ++ph) {
@@ -151,7 +151,7 @@ batched_stream_kernel(BatchWork w,
       const TS* in = ph == 0 ? (const TS*)bg.first_in
                              : (const TS*)(out_dst ? bg.scratch : bg.dst);
       TS* out = out_dst ? (TS*)bg.dst : (TS*)bg.scratch;
-      stream2d_warp_segments<TS, R, R, R, R, STAR, SEG, V, true>(
+      stream2d_warp_segments<TS, R, R, R, R, STAR, SEG, V, true, DF>(
           in, out, bg.w, bg.h, bg.pitch, wx * C::OUT_COLS, 0, bg.h, (int)sgi, 1 << 30, w.bnd,
           cf);
     }
@@ -168,18 +168,19 @@ struct BatchLaunch {
   cudaStream_t stream;
 };
 
-// STREAM: the row-streaming kernel (P = SEG rows per segment, TT = 1).
-template <typename TS, int R, bool STAR, int P, int TT, int V, bool STREAM = false>
+// STREAM: the row-streaming kernel (P = SEG rows per segment, TT = 1, DF
+// rows in flight ahead of the reach).
+template <typename TS, int R, bool STAR, int P, int TT, int V, bool STREAM = false, int DF = 4>
 static int launch_batched(BatchLaunch& a) {
   using TA = typename Traits<TS>::TA;
   using CW = Stencil2DCfg<TS, R, R, R, R, STAR, P, TT, V>;
-  using CS = Stream2DCfg<TS, R, R, R, R, STAR, P, V>;
+  using CS = Stream2DCfg<TS, R, R, R, R, STAR, P, V, DF>;
   constexpr int NC = (2 * R + 1) * (2 * R + 1);
   constexpr int OUT_COLS = STREAM ? CS::OUT_COLS : CW::OUT_COLS;
   constexpr int ROWS = STREAM ? CS::SEGL : P;  // rows of one work item
   static_assert(!STREAM || TT == 1, "streaming tiles take single steps");
   auto kern = [] {
-    if constexpr (STREAM) return &batched_stream_kernel<TS, R, STAR, P, V>;
+    if constexpr (STREAM) return &batched_stream_kernel<TS, R, STAR, P, V, DF>;
     else return &batched_kernel<TS, R, STAR, P, TT, V>;
   }();
   std::vector<BatchGrid>& grids = *a.grids;
@@ -276,30 +277,57 @@ static BatchFn find_batched(int dtype, int star, int r, int t) {
   return nullptr;
 }
 
-// Single-step streaming kernels (SEG = 32) for the same stencils.
-static BatchFn find_batched_stream(int dtype, int star, int r) {
-#define SSAM_BS(TS, R, ST, V) \
-  if (r == R && star == (ST ? 1 : 0)) return &launch_batched<TS, R, ST, 32, 1, V, true>;
-  switch (dtype) {
-    case SSAM_F32:
-      SSAM_BS(float, 1, true, 4) SSAM_BS(float, 1, false, 4)
-      SSAM_BS(float, 2, true, 4) SSAM_BS(float, 2, false, 4)
-      SSAM_BS(float, 3, true, 4) SSAM_BS(float, 3, false, 4)
-      break;
-    case SSAM_F64:
-      SSAM_BS(double, 1, true, 4) SSAM_BS(double, 1, false, 4)
-      SSAM_BS(double, 2, true, 4) SSAM_BS(double, 2, false, 4)
-      break;
-    case SSAM_BF16:
-      SSAM_BS(__nv_bfloat16, 1, true, 8) SSAM_BS(__nv_bfloat16, 1, false, 8)
-      SSAM_BS(__nv_bfloat16, 2, true, 8) SSAM_BS(__nv_bfloat16, 2, false, 8)
-      break;
+// Single-step streaming kernels (SEG = 32) for the same stencils, each with
+// 4, 6 or 8 rows in flight a warp (`depth`): X(TS, R, STAR, V) per stencil.
+#define SSAM_BATCH_STREAM_LIST(X)                                            \
+  switch (dtype) {                                                           \
+    case SSAM_F32:                                                           \
+      X(float, 1, true, 4) X(float, 1, false, 4) X(float, 2, true, 4)        \
+      X(float, 2, false, 4) X(float, 3, true, 4) X(float, 3, false, 4)       \
+      break;                                                                 \
+    case SSAM_F64:                                                           \
+      X(double, 1, true, 4) X(double, 1, false, 4) X(double, 2, true, 4)     \
+      X(double, 2, false, 4)                                                 \
+      break;                                                                 \
+    case SSAM_BF16:                                                          \
+      X(__nv_bfloat16, 1, true, 8) X(__nv_bfloat16, 1, false, 8)             \
+      X(__nv_bfloat16, 2, true, 8) X(__nv_bfloat16, 2, false, 8)             \
+      break;                                                                 \
   }
+
+static BatchFn find_batched_stream(int dtype, int star, int r, int depth) {
+#define SSAM_BS(TS, R, ST, V)                                                \
+  if (r == R && star == (ST ? 1 : 0)) {                                      \
+    if (depth == 4) return &launch_batched<TS, R, ST, 32, 1, V, true, 4>;    \
+    if (depth == 6) return &launch_batched<TS, R, ST, 32, 1, V, true, 6>;    \
+    if (depth == 8) return &launch_batched<TS, R, ST, 32, 1, V, true, 8>;    \
+  }
+  SSAM_BATCH_STREAM_LIST(SSAM_BS)
 #undef SSAM_BS
   return nullptr;
 }
 
+#undef SSAM_BATCH_STREAM_LIST
+
 static int stream_width(int dtype) { return dtype == SSAM_BF16 || dtype == SSAM_F16 ? 8 : 4; }
+
+// Rows in flight a warp for the persistent streaming kernel of this stencil.
+// A deeper ring keeps more loads in flight a warp but takes registers, and
+// the kernel's register count (so its CTAs a SM) does not follow the depth
+// monotonically.  Measured on the 256-grid, 50-step benchmark batches (sides
+// log-uniform in [64, 2048]) with depths 4 / 6 / 8: FP32 5x5 box 286 / 320 /
+// 294 GCells/s, FP32 5-point 539 / 497 / 549, BF16 5-point 623 / 560 / 526,
+// BF16 5x5 box 225 / 196 / 181.  SSAM_BATCH_DEPTH=4|6|8 in the environment
+// pins one depth.
+static int batched_stream_depth(int dtype, int star, int r) {
+  if (const char* e = getenv("SSAM_BATCH_DEPTH")) {
+    const int d = atoi(e);
+    if (d == 4 || d == 6 || d == 8) return d;
+  }
+  if (dtype == SSAM_F32 && r == 2 && !star) return 6;
+  if (dtype == SSAM_F32 && r == 1 && star) return 8;
+  return 4;
+}
 
 }  // namespace ssam
 
@@ -362,7 +390,10 @@ extern "C" int ssam_stencil2d_batched(const ssam_grid2d* grids, int ngrids, int 
                   (uintptr_t)grids[i].dst % 16 == 0 &&
                   grids[i].pitch % stream_width(dtype) == 0 &&
                   (boundary != SSAM_BOUNDARY_CLAMP || grids[i].width % stream_width(dtype) == 0);
-  BatchFn fn_stream = all_aligned ? find_batched_stream(dtype, star, radius) : nullptr;
+  BatchFn fn_stream =
+      all_aligned
+          ? find_batched_stream(dtype, star, radius, batched_stream_depth(dtype, star, radius))
+          : nullptr;
   if (fn_stream) {
     fn_one = fn_stream;
     if (deep == 1) fn_deep = fn_stream;

@@ -177,6 +177,50 @@ struct CoefBlock {
   TA c[N];
 };
 
+// One tap of the own-column part of a 2D stencil row: acc[j] += w * row[j+dx]
+// for every j with 0 <= j + dx < V (dx is a constant once the caller's tap
+// loop is unrolled).  For a float accumulator and an even dx the columns go
+// in pairs through the packed two-lane FP32 FMA (FFMA2): each lane is rounded
+// like a scalar fma, so every sum keeps its bits and its order, with half the
+// FMA instructions.  An odd dx would pair registers across a pair boundary,
+// which costs a move per lane, so it stays scalar.  PAIR = false keeps every
+// tap scalar: the paired form holds more registers, which costs the
+// row-streaming tiles of bandwidth-bound stencils more occupancy than the
+// saved instructions are worth (see pair_taps).
+template <int V, bool PAIR = true, typename TA>
+__device__ __forceinline__ void tap_row(TA (&acc)[V], TA w, const TA* row, int dx) {
+  if constexpr (PAIR && std::is_same<TA, float>::value && V % 2 == 0) {
+    if ((dx & 1) == 0) {
+      const float2 w2 = make_float2(w, w);
+#pragma unroll
+      for (int j = 0; j < V; j += 2) {
+        if (j + dx < 0 || j + dx >= V) continue;  // both lanes of the pair leave together
+        float2 a = make_float2(acc[j], acc[j + 1]);
+        a = __ffma2_rn(w2, make_float2(row[j + dx], row[j + dx + 1]), a);
+        acc[j] = a.x;
+        acc[j + 1] = a.y;
+      }
+      return;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < V; ++j) {
+    if (j + dx < 0 || j + dx >= V) continue;
+    acc[j] = fma(w, row[j + dx], acc[j]);
+  }
+}
+
+// Whether the row-streaming tiles pair their taps: only where the stencil
+// does at least 8 flop per byte of HBM traffic (2*taps-1 flop per cell
+// against a read and a write of the storage type), i.e. where the FMA pipe
+// and not HBM bounds the tile.  Measured on 8192^2 grids: BF16 5x5 box
+// 637 -> 724 GCells/s paired; the FP32 5x5 box and 13-point star lost 15 %
+// paired (more registers, fewer warps in flight).
+template <typename TS, int TAPS>
+__host__ __device__ constexpr bool pair_taps() {
+  return 2 * TAPS - 1 >= 16 * (int)sizeof(TS);
+}
+
 // ---------------------------------------------------------- kernel registry --
 
 // One compiled 2D stencil kernel: radii left/right/top/bottom, tap pattern,

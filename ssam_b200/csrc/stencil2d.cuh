@@ -223,12 +223,7 @@ __device__ __forceinline__ void stencil2d_warp_tile(
 #pragma unroll
         for (int dx = -RL; dx <= RR; ++dx) {
           if (STAR && dy != 0 && dx != 0) continue;
-          const TA w = cf.c[(dy + RT) * FW + (dx + RL)];
-#pragma unroll
-          for (int j = 0; j < V; ++j) {
-            if (j + dx < 0 || j + dx >= V) continue;
-            acc[j] = fma(w, d[i + RT + dy][j + dx], acc[j]);
-          }
+          tap_row<V>(acc, cf.c[(dy + RT) * FW + (dx + RL)], d[i + RT + dy], dx);
         }
       }
       // partial sums travelling right: virtual column V+q, q < RL

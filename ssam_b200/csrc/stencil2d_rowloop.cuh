@@ -94,13 +94,7 @@ stencil2d_rowloop_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int64
 #pragma unroll
         for (int dx = 0; dx < FW; ++dx) w[dx] = cf.c[fy * FW + dx];
 #pragma unroll
-        for (int dx = -RL; dx <= RR; ++dx) {
-#pragma unroll
-          for (int j = 0; j < V; ++j) {
-            if (j + dx < 0 || j + dx >= V) continue;
-            acc[j] = fma(w[dx + RL], d[j + dx], acc[j]);
-          }
-        }
+        for (int dx = -RL; dx <= RR; ++dx) tap_row<V>(acc, w[dx + RL], d, dx);
         if constexpr (RL > 0) {
 #pragma unroll
           for (int q = 0; q < RL; ++q) {

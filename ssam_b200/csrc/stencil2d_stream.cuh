@@ -24,7 +24,7 @@
 
 namespace ssam {
 
-template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int SEG, int V_>
+template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int SEG, int V_, int DF = 0>
 struct Stream2DCfg {
   using TA = typename Traits<TS>::TA;
   static constexpr int V = V_;
@@ -38,8 +38,8 @@ struct Stream2DCfg {
   static constexpr int CH = V * (int)sizeof(TS) / 16;  // 16-byte words per row
   // rows in flight ahead of the reach: 2 KB (FP32/16-bit) or 4 KB (FP64) a
   // warp (one row for reaches of 13 rows and more, whose longer ring the
-  // compiler would otherwise keep in local memory)
-  static constexpr int D = FH >= 13 ? 1 : 4;
+  // compiler would otherwise keep in local memory), or DF rows when given
+  static constexpr int D = DF > 0 ? DF : (FH >= 13 ? 1 : 4);
   static constexpr int L = FH + D;  // ring length = unroll factor
   // rows beyond the ones in flight that are prefetched into L2 (no registers
   // held), so that the loads D rows ahead find their lines on chip
@@ -118,13 +118,13 @@ __device__ __forceinline__ void stream_fix_lane(TA (&d)[V], int where, int nin, 
 // it the launcher guarantees whole chunks and the partial-chunk code is left
 // out of the unrolled ring (it costs registers and instruction fetch).
 template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int SEG, int V_,
-          bool PARTIAL = false>
+          bool PARTIAL = false, int DF = 0>
 __device__ __forceinline__ void stream2d_warp_segments(
     const TS* __restrict__ src, TS* __restrict__ dst, int64_t W, int64_t H, int64_t pitch,
     int64_t x_out0, int64_t y_begin, int64_t y_end, int sg0, int sstride, int bnd,
     const CoefBlock<typename Traits<TS>::TA,
                     Stream2DCfg<TS, RL, RR, RT, RB, STAR, SEG, V_>::NC>& cf) {
-  using C = Stream2DCfg<TS, RL, RR, RT, RB, STAR, SEG, V_>;
+  using C = Stream2DCfg<TS, RL, RR, RT, RB, STAR, SEG, V_, DF>;
   using TA = typename C::TA;
   constexpr int V = C::V, FW = C::FW, FH = C::FH, CH = C::CH, D = C::D, L = C::L,
                 PF = C::PF;
@@ -217,12 +217,8 @@ __device__ __forceinline__ void stream2d_warp_segments(
 #pragma unroll
           for (int dx = -RL; dx <= RR; ++dx) {
             if (STAR && dy != 0 && dx != 0) continue;
-            const TA w = cf.c[(dy + RT) * FW + (dx + RL)];
-#pragma unroll
-            for (int j = 0; j < V; ++j) {
-              if (j + dx < 0 || j + dx >= V) continue;
-              acc[j] = fma(w, val[(u + RT + dy) % L][j + dx], acc[j]);
-            }
+            tap_row<V, pair_taps<TS, STAR ? FW + FH - 1 : FW * FH>()>(
+                acc, cf.c[(dy + RT) * FW + (dx + RL)], val[(u + RT + dy) % L], dx);
           }
         }
         // partial sums travelling right: virtual column V+q, q < RL

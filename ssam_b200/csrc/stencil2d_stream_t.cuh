@@ -50,7 +50,8 @@ struct StreamT2DCfg {
 // sums for the neighbouring lanes' columns moved one lane downstream by
 // shuffle (a chain when a reach exceeds V) -- the products and their order
 // are those of the other 2D tiles.
-template <int RL, int RR, int RT, int RB, bool STAR, int V, int NR, typename TA, int NC>
+template <int RL, int RR, int RT, int RB, bool STAR, int V, int NR, bool PAIR, typename TA,
+          int NC>
 __device__ __forceinline__ void stream_row_sum(TA (&acc)[V], const TA (&ring)[NR][V], int o,
                                                const CoefBlock<TA, NC>& cf) {
   constexpr int FW = RL + RR + 1;
@@ -62,12 +63,7 @@ __device__ __forceinline__ void stream_row_sum(TA (&acc)[V], const TA (&ring)[NR
 #pragma unroll
     for (int dx = -RL; dx <= RR; ++dx) {
       if (STAR && dy != 0 && dx != 0) continue;
-      const TA w = cf.c[(dy + RT) * FW + (dx + RL)];
-#pragma unroll
-      for (int j = 0; j < V; ++j) {
-        if (j + dx < 0 || j + dx >= V) continue;
-        acc[j] = fma(w, ring[(o + RT + dy) % NR][j + dx], acc[j]);
-      }
+      tap_row<V, PAIR>(acc, cf.c[(dy + RT) * FW + (dx + RL)], ring[(o + RT + dy) % NR], dx);
     }
   }
   if constexpr (RL > 0) {
@@ -139,6 +135,7 @@ stencil2d_stream_t_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int6
   using TA = typename C::TA;
   constexpr int V = C::V, FH = C::FH, CH = C::CH, D = C::D, L = C::L, W0 = C::W0,
                 PF = C::PF, SEGL = C::SEGL;
+  constexpr bool PAIR = pair_taps<TS, STAR ? RL + RR + FH : (RL + RR + 1) * FH>();
   const int64_t warp_x = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int64_t x_out0 = warp_x * C::OUT_COLS;
   if (x_out0 >= W) return;  // whole warp leaves together
@@ -234,7 +231,7 @@ stencil2d_stream_t_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int6
 
         // step 1 from the input ring
         TA acc[V];
-        stream_row_sum<RL, RR, RT, RB, STAR, V, L>(acc, val, u, cf);
+        stream_row_sum<RL, RR, RT, RB, STAR, V, L, PAIR>(acc, val, u, cf);
         fix_row(acc, y1);
 #pragma unroll
         for (int j = 0; j < V; ++j) lev[0][u % FH][j] = acc[j];
@@ -243,7 +240,7 @@ stencil2d_stream_t_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int6
 #pragma unroll
         for (int s = 2; s <= T; ++s) {
           const int ys = y1 - (s - 1) * RB;
-          stream_row_sum<RL, RR, RT, RB, STAR, V, FH>(acc, lev[s - 2],
+          stream_row_sum<RL, RR, RT, RB, STAR, V, FH, PAIR>(acc, lev[s - 2],
                                                      (u + 2 * FH - RB - RT) % FH, cf);
           fix_row(acc, ys);
           if (s < T) {

@@ -180,3 +180,36 @@ def test_grid_barrier_that_gives_up_reports_a_timeout(cuda):
         want = oracle.conv2d(h, m, "copy", steps=6)
         assert np.abs(o.cpu().numpy() - want).max() <= 6e-5
 
+
+
+@pytest.mark.parametrize("depth", ["4", "6", "8"])
+@pytest.mark.parametrize("tdt,kind,r", [(torch.float32, "star", 1), (torch.float32, "box", 2),
+                                        (torch.float32, "star", 3), (torch.float64, "box", 2),
+                                        (torch.bfloat16, "star", 1), (torch.bfloat16, "box", 2)])
+def test_batched_stream_depths(cuda, monkeypatch, depth, tdt, kind, r):
+    """Every compiled depth of the persistent streaming kernel (rows in
+    flight a warp; SSAM_BATCH_DEPTH pins one) gives the bits of a chain of
+    single-step per-grid launches (a 16-bit grid is rounded to its storage
+    type after every step there too).  COPY boundary, so that every phase is
+    a single streamed step; 16-byte aligned rows."""
+    monkeypatch.setenv("SSAM_BATCH_DEPTH", depth)
+    hosts = _grids(10, 20, 400, stable_seed(str(tdt), kind, r))
+    if kind == "star":
+        c = normalised((4 * r + 1,), r)
+        shape = S.STAR
+    else:
+        c = normalised((2 * r + 1, 2 * r + 1), r).ravel()
+        shape = S.BOX
+    srcs = []
+    for h in hosts:  # rows pitched to whole 16-byte chunks of 8 columns
+        pitch = -(-h.shape[1] // 8) * 8
+        base = torch.zeros(h.shape[0], pitch, dtype=tdt, device=cuda)
+        base[:, :h.shape[1]] = torch.from_numpy(h).to(tdt)
+        srcs.append(base[:, :h.shape[1]])
+    got = S.stencil2d_batched(srcs, c, r, shape, 5, "copy", persistent=True)
+    ref = srcs
+    for _ in range(5):
+        ref = S.stencil2d_batched(ref, c, r, shape, 1, "copy", persistent=False)
+    S.device_status()
+    for a, b in zip(got, ref):
+        assert torch.equal(a, b), f"depth {depth} {a.shape}"
