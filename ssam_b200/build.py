@@ -90,16 +90,17 @@ def instances_3d():
                          (2, 12, 4, "z"), (2, 16, 4, "z"), (2, 16, 8, "z"), (2, 12, 8, "z"),
                          (2, 8, 4, "z8"), (2, 8, 8, "z8"), (4, 4, 8, "c8")],
                 (1, 1): [(4, 8, 6), (4, 4, 8), (2, 16, 6), (4, 16, 5), (4, 8, 8),
-                         (2, 16, 4, "z"), (2, 8, 4, "z"), (2, 16, 8, "z")],
+                         (2, 16, 4, "z"), (2, 8, 4, "z"), (2, 16, 8, "z"), (4, 8, 8, "z")],
                 "rhs": [(4, 8, 6), (4, 4, 8), (2, 16, 6), (4, 16, 5),
-                        (2, 16, 4, "z"), (2, 8, 4, "z"), (2, 16, 8, "z"), (2, 8, 8, "z")]},
+                        (2, 16, 4, "z"), (2, 8, 4, "z"), (2, 16, 8, "z"), (2, 8, 8, "z"),
+                        (4, 12, 8, "z")]},
         "bf16": {(0, 1): [(4, 8, 6), (2, 16, 6), (4, 16, 6), (8, 8, 6), (2, 16, 4, "z"),
                           (2, 16, 8, "z"), (4, 12, 8, "z"), (2, 8, 4, "z8"), (4, 8, 6, "c8")],
                  (0, 2): [(4, 4, 8), (4, 8, 6), (2, 16, 6), (2, 12, 4, "z"), (2, 16, 8, "z"),
                           (2, 8, 4, "z8"), (2, 8, 8, "z8"), (4, 4, 8, "c8")],
                  (1, 1): [(4, 8, 6), (2, 16, 6), (4, 16, 6), (2, 16, 4, "z"), (2, 16, 8, "z")],
                  "rhs": [(4, 8, 6), (2, 16, 6), (4, 16, 6), (2, 16, 4, "z"), (2, 8, 4, "z"),
-                         (2, 16, 8, "z")]},
+                         (2, 16, 8, "z"), (4, 12, 8, "z")]},
         "f64": {(0, 1): [(4, 4, 5), (4, 8, 5), (2, 8, 5), (2, 4, 4, "z"), (2, 8, 8, "z")],
                 (0, 2): [(4, 4, 6), (2, 8, 6), (2, 4, 4, "z"), (2, 8, 8, "z")],
                 (1, 1): [(4, 4, 5), (2, 8, 5), (2, 4, 4, "z"), (2, 8, 8, "z")],
