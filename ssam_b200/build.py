@@ -97,7 +97,7 @@ def instances_3d():
         "bf16": {(0, 1): [(4, 8, 6), (2, 16, 6), (4, 16, 6), (8, 8, 6), (2, 16, 4, "z"),
                           (2, 16, 8, "z"), (4, 12, 8, "z"), (2, 8, 4, "z8"), (4, 8, 6, "c8")],
                  (0, 2): [(4, 4, 8), (4, 8, 6), (2, 16, 6), (2, 12, 4, "z"), (2, 16, 8, "z"),
-                          (2, 8, 4, "z8"), (2, 8, 8, "z8"), (4, 4, 8, "c8")],
+                          (2, 8, 4, "z8"), (2, 8, 8, "z8"), (4, 4, 8, "c8"), (2, 12, 8, "z")],
                  (1, 1): [(4, 8, 6), (2, 16, 6), (4, 16, 6), (2, 16, 4, "z"), (2, 16, 8, "z")],
                  "rhs": [(4, 8, 6), (2, 16, 6), (4, 16, 6), (2, 16, 4, "z"), (2, 8, 4, "z"),
                          (2, 16, 8, "z"), (4, 12, 8, "z")]},

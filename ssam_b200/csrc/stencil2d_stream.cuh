@@ -37,9 +37,10 @@ struct Stream2DCfg {
   static constexpr int OUT_COLS = OUT_LANES * V;
   static constexpr int CH = V * (int)sizeof(TS) / 16;  // 16-byte words per row
   // rows in flight ahead of the reach: 2 KB (FP32/16-bit) or 4 KB (FP64) a
-  // warp (one row for reaches of 13 rows and more, whose longer ring the
-  // compiler would otherwise keep in local memory), or DF rows when given
-  static constexpr int D = DF > 0 ? DF : (FH >= 13 ? 1 : 4);
+  // warp, or DF rows when given.  (The 13-row reach of the 25-point star
+  // takes 4 too: with 1 its ring needed 128 registers and spilled, with 4 it
+  // holds 68 -- 110 / 80 for BF16, 178 / 128 for FP64.)
+  static constexpr int D = DF > 0 ? DF : 4;
   static constexpr int L = FH + D;  // ring length = unroll factor
   // rows beyond the ones in flight that are prefetched into L2 (no registers
   // held), so that the loads D rows ahead find their lines on chip

@@ -255,6 +255,34 @@ def test_config2_conv21_8192_sampled_rows(cuda):
     _slab_check(out, src, w, [0, 9, 10, 4000, n - 11, n - 1], np.float32, "conv21")
 
 
+@pytest.mark.parametrize("dt,r", [("f32", 1), ("f32", 2), ("f32", 3), ("f64", 1)])
+def test_config2_sixteen_steps_8192_vs_oracle_rows(cuda, dt, r):
+    """Config 2's 16-step run at its full size (8192^2, uniform[-1,1), box
+    coefficients normalised to 1, zero padding), in the launch chain the
+    autotuner picks for it (temporal blocking included), against the oracle
+    on row slabs carrying 16r rows of halo on each side: rows that far from
+    a slab cut see exactly the whole grid's values."""
+    n, steps = 8192, 16
+    npdt = DT[dt]
+    src = uniform((n, n), -1, 1, npdt, 16000 + r)
+    m = normalised((2 * r + 1, 2 * r + 1), 160 + r)
+    x = dev(src, cuda)
+    S.autotune_clear()
+    try:
+        S.autotune_stencil2d(x, m.ravel(), r, S.BOX, steps=steps)
+        out = host(S.stencil2d(x, m.ravel(), r, S.BOX, steps=steps))
+        S.device_status()
+    finally:
+        S.autotune_clear()
+    halo = r * steps
+    for y in [0, 1, halo, n // 2, n - 2, n - 1] + list(rng(r).integers(0, n, 3)):
+        lo, hi = max(0, y - halo), min(n, y + halo + 1)
+        slab = np.ascontiguousarray(src[lo:hi])
+        want = oracle.conv2d(slab, m.astype(npdt), "zero", steps=steps)[y - lo]
+        scale = magnitude2d(slab, m, "zero", steps)[y - lo]
+        assert_rel_close(out[y], want, scale, REL[npdt] * steps, f"{dt} box{r} row {y}")
+
+
 def test_sixteen_steps_8192_invariants(cuda):
     """16 steps of a normalised box on a constant field stay constant in the
     interior and the copied ring stays untouched (size-independent checks)."""

@@ -292,3 +292,56 @@ def test_512_bf16_100_steps_vs_fp64_oracle(cuda, tmp_path):
         print(f"bf16 512^3 100 steps, {depth} step(s) a launch, vs FP64 oracle: max abs "
               f"{amax:.3e}, rms {rms:.3e}, max scaled {worst:.3e}")
         assert amax <= 0.05 and rms <= 0.01
+
+
+@pytest.mark.parametrize("kind", ["13pt", "19pt"])
+def test_512_autotuned_single_step_vs_oracle_slabs(cuda, kind):
+    """512^3 FP32, the configuration the autotuner picks for the benchmark
+    (one step a launch) against the oracle on z-slabs at both faces and
+    inside, one step and a 4-step chain."""
+    n = 512
+    g = torch.Generator(device=cuda)
+    g.manual_seed(13)
+    x = torch.rand(n, n, n, device=cuda, generator=g)
+    if kind == "19pt":
+        cube, sh, r = poisson_cube(), S.POISSON19, 1
+        cube = cube / np.abs(cube).sum()
+    else:
+        cube, sh, r = cube_from_taps(taps_j3d13pt(), 2), S.STAR3D, 2
+        cube = cube / np.abs(cube).sum()
+    S.autotune_clear()
+    try:
+        S.autotune_stencil3d(x, cube, r, sh, boundary="copy")
+        outs = {k: S.stencil3d(x, cube, r, sh, steps=k, boundary="copy").cpu().numpy()
+                for k in (1, 4)}
+        S.device_status()
+    finally:
+        S.autotune_clear()
+    xs = x.cpu().numpy()
+    for k, o in outs.items():
+        slab_check(xs, o, cube, k, (0, 1, 2, 255, 509, 510, 511), "copy", 1e-5 * k)
+
+
+def test_512_bf16_13pt_100_steps_vs_fp64_oracle(cuda):
+    """The benchmark's BF16-storage 13-point run (512^3, 100 steps in one CUDA
+    graph, the autotuned kernel) against the FP64 oracle on z-slabs; states
+    the max and RMS error."""
+    n, steps = 512, 100
+    g = torch.Generator(device=cuda)
+    g.manual_seed(17)
+    x = torch.rand(n, n, n, device=cuda, generator=g).to(torch.bfloat16)
+    cube = cube_from_taps(taps_j3d13pt(), 2)
+    cube = cube / np.abs(cube).sum()
+    S.autotune_clear()
+    try:
+        S.autotune_stencil3d(x, cube, 2, S.STAR3D, boundary="copy")
+        o = S.stencil3d(x, cube, 2, S.STAR3D, steps=steps, boundary="copy")
+        S.device_status()
+    finally:
+        S.autotune_clear()
+    o = o.double().cpu().numpy()
+    worst, amax, rms = slab_check(x.double().cpu().numpy(), o, cube, steps, (0, 300),
+                                  "copy", steps * 2.0**-8)
+    print(f"bf16 512^3 13-point 100 steps vs FP64 oracle: max abs {amax:.3e}, "
+          f"rms {rms:.3e}, max scaled {worst:.3e}")
+    assert amax <= 0.05 and rms <= 0.01
