@@ -14,11 +14,10 @@
 // wait is bounded by %globaltimer and records an error code on expiry (read
 // with ssam_device_status), so a lost CTA cannot hang the GPU.
 #include <atomic>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
-#include <map>
-#include <mutex>
 #include <string>
 #include <vector>
 
