@@ -135,6 +135,18 @@ __device__ __forceinline__ uint64_t gtimer() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
+// Programmatic dependent launch: a 3D launch may begin while the launch
+// before it in the stream is finishing (the launcher sets
+// cudaLaunchAttributeProgrammaticStreamSerialization).  Called by every
+// thread after the shared-memory set-up, before any global memory access:
+// the wait returns once the previous grid has completed and its writes are
+// visible (at once when there is no such grid), and the release then lets
+// the next launch of the stream start its own set-up on SMs this grid frees.
+__device__ __forceinline__ void pdl_wait_then_release() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 __device__ __forceinline__ void mbar_init(uint64_t* b, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count)
                : "memory");
@@ -384,6 +396,7 @@ stencil3d_kernel(const __grid_constant__ CUtensorMap map, const TS* __restrict__
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
+  pdl_wait_then_release();
 
   const int64_t nx = w.nx, ny = w.ny, nz = w.nz, nxy = nx * ny;
 

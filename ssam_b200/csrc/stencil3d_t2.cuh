@@ -164,6 +164,7 @@ stencil3d_t2_kernel(const __grid_constant__ CUtensorMap map, const TS* __restric
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
+  pdl_wait_then_release();
 
   const int64_t nx = w.nx, ny = w.ny, nz = w.nz, nxy = nx * ny;
 
