@@ -170,6 +170,36 @@ __device__ __forceinline__ void store_vec(TS* __restrict__ p, const TA (&r)[V]) 
   }
 }
 
+// Programmatic dependent launch.  The 2D and 3D stencil kernels are
+// launched with cudaLaunchAttributeProgrammaticStreamSerialization
+// (launch_pdl), so that a launch may begin while the launch before it in the
+// stream is finishing.  Every thread of such a kernel calls this before its
+// first global memory access (the 3D kernels after their shared-memory
+// set-up): the wait returns once the previous grid has completed and its
+// writes are visible (at once when there is none), and the release then lets
+// the next launch of the stream start on SMs this grid frees.
+__device__ __forceinline__ void pdl_wait_then_release() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                       cudaStream_t stream, Args&&... args) {
+  cudaLaunchConfig_t lc;
+  memset(&lc, 0, sizeof(lc));
+  lc.gridDim = grid;
+  lc.blockDim = block;
+  lc.dynamicSmemBytes = smem;
+  lc.stream = stream;
+  cudaLaunchAttribute la[1];
+  la[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  la[0].val.programmaticStreamSerializationAllowed = 1;
+  lc.attrs = la;
+  lc.numAttrs = 1;
+  return cudaLaunchKernelEx(&lc, kern, static_cast<Args&&>(args)...);
+}
+
 // Coefficients passed by value as a kernel parameter (constant bank), indexed
 // with compile-time offsets by the unrolled kernels.
 template <typename TA, int N>

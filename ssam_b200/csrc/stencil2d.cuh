@@ -340,6 +340,7 @@ stencil2d_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int64_t W,
                  CoefBlock<typename Traits<TS>::TA,
                            Stencil2DCfg<TS, RL, RR, RT, RB, STAR, P, T, V_>::NC> cf) {
   using C = Stencil2DCfg<TS, RL, RR, RT, RB, STAR, P, T, V_>;
+  pdl_wait_then_release();
   const int64_t warp_x = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int64_t x_out0 = warp_x * C::OUT_COLS;
   if (x_out0 >= W) return;  // whole warp leaves together
@@ -361,11 +362,12 @@ cudaError_t launch_stencil2d(const Launch2D& a) {
   dim3 grid((unsigned)((warps_x + nw - 1) / nw), (unsigned)(nby < 65535 ? nby : 65535));
   const int vec_ok = ((uintptr_t)a.src % 16 == 0) && ((uintptr_t)a.dst % 16 == 0) &&
                      (a.pitch % C::V == 0);
-  stencil2d_kernel<TS, RL, RR, RT, RB, STAR, P, T, V_><<<grid, 32 * nw, 0, a.stream>>>(
-      (const TS*)a.src, (TS*)a.dst, a.width, a.height, a.pitch, a.y_begin, a.y_end,
-      a.boundary, vec_ok, cf);
+  const cudaError_t e =
+      launch_pdl(&stencil2d_kernel<TS, RL, RR, RT, RB, STAR, P, T, V_>, grid, dim3(32 * nw), 0,
+                 a.stream, (const TS*)a.src, (TS*)a.dst, a.width, a.height, a.pitch,
+                 a.y_begin, a.y_end, a.boundary, vec_ok, cf);
   count_launch();
-  return cudaGetLastError();
+  return e;
 }
 
 template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int P, int T, int V_>

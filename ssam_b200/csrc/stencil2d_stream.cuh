@@ -306,6 +306,7 @@ stencil2d_stream_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int64_
                         CoefBlock<typename Traits<TS>::TA,
                                   Stream2DCfg<TS, RL, RR, RT, RB, STAR, SEG, V_>::NC> cf) {
   using C = Stream2DCfg<TS, RL, RR, RT, RB, STAR, SEG, V_>;
+  pdl_wait_then_release();
   const int64_t warp_x = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int64_t x_out0 = warp_x * C::OUT_COLS;
   if (x_out0 >= W) return;  // whole warp leaves together
@@ -332,11 +333,12 @@ cudaError_t launch_stencil2d_stream(const Launch2D& a) {
     if (!w) return cudaErrorInvalidValue;
     return w->launch(a);
   }
-  stencil2d_stream_kernel<TS, RL, RR, RT, RB, STAR, SEG, V_><<<grid, 32 * nw, 0, a.stream>>>(
-      (const TS*)a.src, (TS*)a.dst, a.width, a.height, a.pitch, a.y_begin, a.y_end,
-      a.boundary, cf);
+  const cudaError_t e =
+      launch_pdl(&stencil2d_stream_kernel<TS, RL, RR, RT, RB, STAR, SEG, V_>, grid,
+                 dim3(32 * nw), 0, a.stream, (const TS*)a.src, (TS*)a.dst, a.width, a.height,
+                 a.pitch, a.y_begin, a.y_end, a.boundary, cf);
   count_launch();
-  return cudaGetLastError();
+  return e;
 }
 
 template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int SEG, int V_>

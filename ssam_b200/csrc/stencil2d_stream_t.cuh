@@ -136,6 +136,7 @@ stencil2d_stream_t_kernel(const TS* __restrict__ src, TS* __restrict__ dst, int6
   constexpr int V = C::V, FH = C::FH, CH = C::CH, D = C::D, L = C::L, W0 = C::W0,
                 PF = C::PF, SEGL = C::SEGL;
   constexpr bool PAIR = pair_taps<TS, STAR ? RL + RR + FH : (RL + RR + 1) * FH>();
+  pdl_wait_then_release();
   const int64_t warp_x = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int64_t x_out0 = warp_x * C::OUT_COLS;
   if (x_out0 >= W) return;  // whole warp leaves together
@@ -277,11 +278,12 @@ cudaError_t launch_stencil2d_stream_t(const Launch2D& a) {
   const int64_t warps_x = (a.width + C::OUT_COLS - 1) / C::OUT_COLS;
   const int64_t nseg = (a.y_end - a.y_begin + C::SEGL - 1) / C::SEGL;
   dim3 grid((unsigned)((warps_x + nw - 1) / nw), (unsigned)(nseg < 65535 ? nseg : 65535));
-  stencil2d_stream_t_kernel<TS, RL, RR, RT, RB, STAR, SEG, V_, T>
-      <<<grid, 32 * nw, 0, a.stream>>>((const TS*)a.src, (TS*)a.dst, a.width, a.height, a.pitch,
-                                       a.y_begin, a.y_end, a.boundary, cf);
+  const cudaError_t e =
+      launch_pdl(&stencil2d_stream_t_kernel<TS, RL, RR, RT, RB, STAR, SEG, V_, T>, grid,
+                 dim3(32 * nw), 0, a.stream, (const TS*)a.src, (TS*)a.dst, a.width, a.height,
+                 a.pitch, a.y_begin, a.y_end, a.boundary, cf);
   count_launch();
-  return cudaGetLastError();
+  return e;
 }
 
 template <typename TS, int RL, int RR, int RT, int RB, bool STAR, int SEG, int V_, int T>

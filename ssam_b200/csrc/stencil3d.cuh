@@ -135,18 +135,6 @@ __device__ __forceinline__ uint64_t gtimer() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// Programmatic dependent launch: a 3D launch may begin while the launch
-// before it in the stream is finishing (the launcher sets
-// cudaLaunchAttributeProgrammaticStreamSerialization).  Called by every
-// thread after the shared-memory set-up, before any global memory access:
-// the wait returns once the previous grid has completed and its writes are
-// visible (at once when there is no such grid), and the release then lets
-// the next launch of the stream start its own set-up on SMs this grid frees.
-__device__ __forceinline__ void pdl_wait_then_release() {
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
-
 __device__ __forceinline__ void mbar_init(uint64_t* b, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count)
                : "memory");

@@ -153,20 +153,9 @@ int launch_3d(const Launch3D& a) {
   CoefBlock<TA, C::NC> cf;
   for (int k = 0; k < C::NC; ++k) cf.c[k] = (TA)a.coef[k];
   // programmatic dependent launch: this grid's set-up may overlap the tail
-  // of the launch before it (the kernel waits for that launch before its
-  // first global memory access; pdl_wait_then_release)
-  cudaLaunchConfig_t lc;
-  memset(&lc, 0, sizeof(lc));
-  lc.gridDim = dim3((unsigned)grid);
-  lc.blockDim = dim3(C::THREADS);
-  lc.dynamicSmemBytes = SMEM;
-  lc.stream = a.stream;
-  cudaLaunchAttribute la[1];
-  la[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  la[0].val.programmaticStreamSerializationAllowed = 1;
-  lc.attrs = la;
-  lc.numAttrs = 1;
-  SSAM_CUDA_TRY(cudaLaunchKernelEx(&lc, kern, map, (const TS*)a.src, (TS*)a.dst, w, cf));
+  // of the launch before it (pdl_wait_then_release in the kernel)
+  SSAM_CUDA_TRY(launch_pdl(kern, dim3((unsigned)grid), dim3(C::THREADS), SMEM, a.stream, map,
+                           (const TS*)a.src, (TS*)a.dst, w, cf));
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   cudaStreamIsCapturing(a.stream, &cap);
   if (cap == cudaStreamCaptureStatusNone) count_launch();  // graphs count at replay
