@@ -64,6 +64,7 @@ struct ConvArgs {
   float out_scale;
   int ci_total, ci_off;         // this pass uses input channels ci_off .. +15
   int n, dil, ty, xp, tiles, nyb, nzc, zc, box_rows, slab, slots;
+  int tmem_cols;                // TMEM columns a CTA allocates (512, or 256 at 2 CTAs a SM)
   int64_t half;                 // elements per half-plane: nb * n^3 * 8
   int64_t items;
   int* err;
@@ -72,6 +73,7 @@ struct ConvArgs {
 
 struct Plan {
   int ty, xp, tiles, box_rows, slab, slots, smem;
+  int ctas_per_sm = 1;
 };
 
 // Largest TY (rows per item) with at most kMaxTiles MMA tiles per output
@@ -386,6 +388,28 @@ bool make_plan_zs(int n, Plan* p) {
   return false;
 }
 
+// Two CTAs a SM: fewer rows a work item (at most 5 tiles = 240 of 256 TMEM
+// columns, at most 113 KB of shared memory), so that two MMA-issuing CTAs
+// share each SM's tensor pipe.
+bool make_plan_zs2(int n, Plan* p) {
+  const int xp = n + 1;
+  if (n > kMaxRow) return false;
+  for (int ty = std::min(n, 16); ty >= 1; ty /= 2) {
+    const int box_rows = ty + 2;
+    const int tiles = (ty * xp + 127) / 128;
+    if (tiles > 5) continue;
+    const int tail = tiles * 128 - ty * xp + 1;
+    const int slab = ((kFrontGuard + box_rows * xp + tail) * 16 + 127) / 128 * 128;
+    const int avail = 113 * 1024 - 1024 - kZsWBytes - 512;
+    const int slots = std::min(kMaxSlots, avail / (2 * slab));
+    if (slots < 2) continue;
+    const int smem = 1024 + kZsWBytes + slots * 2 * slab + 512;
+    *p = Plan{ty, xp, tiles, box_rows, slab, slots, smem, 2};
+    return true;
+  }
+  return false;
+}
+
 __global__ void __launch_bounds__(kThreads, 1) conv3d_zstack_kernel(ConvArgs a) {
   constexpr uint32_t IDESC = tc::idesc_bf16(128, 48, 0, 0);
   extern __shared__ unsigned char smem_raw[];
@@ -431,7 +455,7 @@ __global__ void __launch_bounds__(kThreads, 1) conv3d_zstack_kernel(ConvArgs a) 
     tc::mbar_init(drain, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 1) tc::tmem_alloc(tmem_slot, 512);
+  if (warp == 1) tc::tmem_alloc(tmem_slot, (uint32_t)a.tmem_cols);
   tc::fence_async_smem();
   tc::tc_fence_before();
   __syncthreads();
@@ -586,7 +610,7 @@ __global__ void __launch_bounds__(kThreads, 1) conv3d_zstack_kernel(ConvArgs a) 
   tc::tc_fence_before();
   __syncthreads();
   tc::tc_fence_after();
-  if (warp == 1) tc::tmem_free(tmem, 512);
+  if (warp == 1) tc::tmem_free(tmem, (uint32_t)a.tmem_cols);
 }
 
 }  // namespace
@@ -601,7 +625,12 @@ int conv3d_ring(const void* in, const void* addend, const void* w, int ci_total,
   // (to check the two against each other)
   const char* e27 = getenv("SSAM_CONV_RING27");
   const bool ring27 = e27 && e27[0] == '1';
-  const bool zstack = dil == 1 && !ring27 && make_plan_zs(n, &p);
+  // two CTAs a SM by default (two MMA-issuing CTAs share the tensor pipe:
+  // 8 x 128^3 forward 4.62 -> 3.18 ms); SSAM_CONV_TWO_CTA=0 keeps one
+  const char* e2 = getenv("SSAM_CONV_TWO_CTA");
+  const bool two = !(e2 && e2[0] == '0');
+  const bool zstack =
+      dil == 1 && !ring27 && ((two && make_plan_zs2(n, &p)) || make_plan_zs(n, &p));
   if (!zstack && !make_plan(n, dil, &p)) return SSAM_ERR_UNSUPPORTED;
   ConvArgs a;
   a.in = (const __nv_bfloat16*)in;
@@ -619,6 +648,7 @@ int conv3d_ring(const void* in, const void* addend, const void* w, int ci_total,
   a.box_rows = p.box_rows;
   a.slab = p.slab;
   a.slots = p.slots;
+  a.tmem_cols = p.ctas_per_sm == 2 ? 256 : 512;
   a.nyb = (n + p.ty - 1) / p.ty;
   a.half = (int64_t)nb * n * n * n * 8;
   a.wait_ns = 1000ull * 1000ull * 1000ull;
@@ -633,7 +663,8 @@ int conv3d_ring(const void* in, const void* addend, const void* w, int ci_total,
   for (int nzc = 1; nzc <= n; nzc *= 2) {
     const int zc = (n + nzc - 1) / nzc;
     const int64_t items = cols * nzc;
-    const int64_t rounds = (items + sms - 1) / sms;
+    const int64_t slots_all = (int64_t)sms * p.ctas_per_sm;
+    const int64_t rounds = (items + slots_all - 1) / slots_all;
     const int64_t cost = rounds * (dil == 1 ? zc + 2 : 3 * zc);
     if (best < 0 || cost < best) {
       best = cost;
@@ -650,7 +681,7 @@ int conv3d_ring(const void* in, const void* addend, const void* w, int ci_total,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimit));
     attr_set = true;
   }
-  const int64_t grid = std::min<int64_t>(a.items, sms);
+  const int64_t grid = std::min<int64_t>(a.items, (int64_t)sms * p.ctas_per_sm);
   if (zstack)
     conv3d_zstack_kernel<<<(unsigned)grid, kThreads, p.smem, s>>>(a);
   else
