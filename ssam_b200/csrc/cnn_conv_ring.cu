@@ -410,7 +410,13 @@ bool make_plan_zs2(int n, Plan* p) {
   return false;
 }
 
-__global__ void __launch_bounds__(kThreads, 1) conv3d_zstack_kernel(ConvArgs a) {
+// NI MMA-issuing warps (1 .. 4): warp 0 producer, warps 1 .. NI issue the
+// MMAs of tiles t = i, i + NI, ... (each tile's handshake stays with one
+// issuer; a plane's slot and the final drain wait for all NI), warps NI+1 ..
+// NI+4 the epilogue.
+template <int NI>
+__global__ void __launch_bounds__(32 * (5 + NI), 1) conv3d_zstack_kernel(ConvArgs a) {
+  constexpr int NT = 32 * (5 + NI);
   constexpr uint32_t IDESC = tc::idesc_bf16(128, 48, 0, 0);
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -432,7 +438,7 @@ __global__ void __launch_bounds__(kThreads, 1) conv3d_zstack_kernel(ConvArgs a) 
   // row 16k + co is output channel co of slot k, whose output plane is the
   // one of z-1, z, z+1 that is k mod 3, so its z tap is
   // dz = +1, 0, -1 for (rot - k) mod 3 = 1, 0, 2 (tap index dz + 1).
-  for (int idx = threadIdx.x; idx < 3 * 9 * 48 * 2; idx += kThreads) {
+  for (int idx = threadIdx.x; idx < 3 * 9 * 48 * 2; idx += NT) {
     const int c = idx & 1, row = (idx >> 1) % 48, rt = (idx >> 1) / 48;
     const int rot = rt / 9, t9 = rt % 9, k = row >> 4, co = row & 15;
     const int m = ((rot - k) % 3 + 3) % 3;
@@ -441,18 +447,18 @@ __global__ void __launch_bounds__(kThreads, 1) conv3d_zstack_kernel(ConvArgs a) 
         a.w + ((size_t)co * 27 + tz * 9 + t9) * a.ci_total + a.ci_off + c * 8);
     *reinterpret_cast<uint4*>(Ws + rt * 1536 + (row >> 3) * 256 + c * 128 + (row & 7) * 16) = v;
   }
-  for (int idx = threadIdx.x; idx < S * slot_bytes / 16; idx += kThreads)
+  for (int idx = threadIdx.x; idx < S * slot_bytes / 16; idx += NT)
     reinterpret_cast<uint4*>(Ring)[idx] = make_uint4(0, 0, 0, 0);
   if (threadIdx.x == 0) {
     for (int i = 0; i < S; ++i) {
       tc::mbar_init(&full[i], 1);
-      tc::mbar_init(&empty[i], 1);
+      tc::mbar_init(&empty[i], NI);
     }
     for (int i = 0; i < kZsMaxTiles; ++i) {
       tc::mbar_init(&accf[i], 1);
       tc::mbar_init(&acce[i], 128);
     }
-    tc::mbar_init(drain, 1);
+    tc::mbar_init(drain, NI);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) tc::tmem_alloc(tmem_slot, (uint32_t)a.tmem_cols);
@@ -501,8 +507,9 @@ __global__ void __launch_bounds__(kThreads, 1) conv3d_zstack_kernel(ConvArgs a) 
     if (lane == 0)
       for (uint32_t k = gp > (uint32_t)S ? gp - S : 0; k < gp; ++k)
         if (!tc::mbar_wait(&full[k % S], (k / S) & 1, a.wait_ns)) ok = false;
-  } else if (warp == 1) {
-    // ---------------------------------------------------------- MMA issuer
+  } else if (warp <= NI) {
+    // ---------------------------------------------------------- MMA issuers
+    const int me = warp - 1;
     if (lane == 0) {
       int toff[9];
 #pragma unroll
@@ -524,7 +531,7 @@ __global__ void __launch_bounds__(kThreads, 1) conv3d_zstack_kernel(ConvArgs a) 
           const int rot = (m.z0 - 1 + p + 3) % 3;
           const uint64_t ap = abase0 + (uint64_t)((gp % S) * (slot_bytes >> 4));
           const uint64_t wr = wbase + (uint64_t)(rot * 9 * 96);
-          for (int t = 0; t < T; ++t) {
+          for (int t = me; t < T; t += NI) {
             // slot (z+1) mod 3 of this tile is drained and zeroed
             if (pc > 0 && !tc::mbar_wait(&acce[t], (pc - 1) & 1, a.wait_ns)) {
               ok = false;
@@ -544,10 +551,10 @@ __global__ void __launch_bounds__(kThreads, 1) conv3d_zstack_kernel(ConvArgs a) 
           tc::mma_commit(&empty[gp % S]);  // the plane is read by this plane's MMAs only
         }
       }
-      if (issued) {
-        tc::mma_commit(drain);
-        if (!tc::mbar_wait(drain, 0, a.wait_ns)) ok = false;
-      }
+      // every issuer arrives once; its MMAs must finish before TMEM is freed
+      if (issued) tc::mma_commit(drain);
+      else mbar_arrive(drain);
+      if (!tc::mbar_wait(drain, 0, a.wait_ns)) ok = false;
     }
   } else {
     // ---------------------------------------------------------- epilogue
@@ -631,6 +638,12 @@ int conv3d_ring(const void* in, const void* addend, const void* w, int ci_total,
   const bool two = !(e2 && e2[0] == '0');
   const bool zstack =
       dil == 1 && !ring27 && ((two && make_plan_zs2(n, &p)) || make_plan_zs(n, &p));
+  // MMA-issuing warps of the z-stacked kernel: 2 by default (8 x 128^3
+  // forward at two CTAs a SM, 1 / 2 / 3 / 4 issuers: 3.19 / 2.88 / 2.85 /
+  // 2.84 ms); SSAM_CONV_ISSUERS=1..4 pins one; never more than tiles
+  const char* ei = getenv("SSAM_CONV_ISSUERS");
+  int issuers = (ei && ei[0] >= '1' && ei[0] <= '4') ? ei[0] - '0' : 2;
+  issuers = std::min(issuers, p.tiles);
   if (!zstack && !make_plan(n, dil, &p)) return SSAM_ERR_UNSUPPORTED;
   ConvArgs a;
   a.in = (const __nv_bfloat16*)in;
@@ -677,13 +690,25 @@ int conv3d_ring(const void* in, const void* addend, const void* w, int ci_total,
   if (!attr_set) {
     SSAM_CUDA_TRY(cudaFuncSetAttribute(conv3d_ring_kernel,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimit));
-    SSAM_CUDA_TRY(cudaFuncSetAttribute(conv3d_zstack_kernel,
+    SSAM_CUDA_TRY(cudaFuncSetAttribute(conv3d_zstack_kernel<1>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimit));
+    SSAM_CUDA_TRY(cudaFuncSetAttribute(conv3d_zstack_kernel<2>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimit));
+    SSAM_CUDA_TRY(cudaFuncSetAttribute(conv3d_zstack_kernel<3>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimit));
+    SSAM_CUDA_TRY(cudaFuncSetAttribute(conv3d_zstack_kernel<4>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimit));
     attr_set = true;
   }
   const int64_t grid = std::min<int64_t>(a.items, (int64_t)sms * p.ctas_per_sm);
-  if (zstack)
-    conv3d_zstack_kernel<<<(unsigned)grid, kThreads, p.smem, s>>>(a);
+  if (zstack && issuers == 4)
+    conv3d_zstack_kernel<4><<<(unsigned)grid, 32 * 9, p.smem, s>>>(a);
+  else if (zstack && issuers == 3)
+    conv3d_zstack_kernel<3><<<(unsigned)grid, 32 * 8, p.smem, s>>>(a);
+  else if (zstack && issuers == 2)
+    conv3d_zstack_kernel<2><<<(unsigned)grid, 32 * 7, p.smem, s>>>(a);
+  else if (zstack)
+    conv3d_zstack_kernel<1><<<(unsigned)grid, 32 * 6, p.smem, s>>>(a);
   else
     conv3d_ring_kernel<<<(unsigned)grid, kThreads, p.smem, s>>>(a);
   count_launch();
