@@ -414,9 +414,11 @@ bool make_plan_zs2(int n, Plan* p) {
 // MMAs of tiles t = i, i + NI, ... (each tile's handshake stays with one
 // issuer; a plane's slot and the final drain wait for all NI), warps NI+1 ..
 // NI+4 the epilogue.
-template <int NI>
-__global__ void __launch_bounds__(32 * (5 + NI), 1) conv3d_zstack_kernel(ConvArgs a) {
-  constexpr int NT = 32 * (5 + NI);
+// NE epilogue groups of 4 warps (one a TMEM lane quarter); group g drains
+// the tiles t = g, g + NE, ...
+template <int NI, int NE = 1>
+__global__ void __launch_bounds__(32 * (1 + NI + 4 * NE), 1) conv3d_zstack_kernel(ConvArgs a) {
+  constexpr int NT = 32 * (1 + NI + 4 * NE);
   constexpr uint32_t IDESC = tc::idesc_bf16(128, 48, 0, 0);
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -559,6 +561,7 @@ __global__ void __launch_bounds__(32 * (5 + NI), 1) conv3d_zstack_kernel(ConvArg
   } else {
     // ---------------------------------------------------------- epilogue
     const int q = warp & 3;
+    const int grp = (warp - 1 - NI) >> 2;  // epilogue group (4 consecutive warps)
     const int row = q * 32 + lane;
     const uint32_t lanes = (uint32_t)(q * 32) << 16;
     uint32_t pc = 0;
@@ -569,7 +572,7 @@ __global__ void __launch_bounds__(32 * (5 + NI), 1) conv3d_zstack_kernel(ConvArg
         const bool store = p >= 2;    // zo in z0 .. z0 + nout - 1
         const int k = (zo + 3) % 3;
         const int64_t zrow = ((int64_t)m.b * n + zo) * n;
-        for (int t = 0; t < T; ++t) {
+        for (int t = grp; t < T; t += NE) {
           // (warp-uniform, for the .sync.aligned TMEM accesses below)
           const bool got = tc::mbar_wait(&accf[t], pc & 1, a.wait_ns);
           if (!__all_sync(0xffffffffu, got)) {
@@ -638,11 +641,12 @@ int conv3d_ring(const void* in, const void* addend, const void* w, int ci_total,
   const bool two = !(e2 && e2[0] == '0');
   const bool zstack =
       dil == 1 && !ring27 && ((two && make_plan_zs2(n, &p)) || make_plan_zs(n, &p));
-  // MMA-issuing warps of the z-stacked kernel: 2 by default (8 x 128^3
+  // MMA-issuing warps of the z-stacked kernel: 3 by default (8 x 128^3
   // forward at two CTAs a SM, 1 / 2 / 3 / 4 issuers: 3.19 / 2.88 / 2.85 /
-  // 2.84 ms); SSAM_CONV_ISSUERS=1..4 pins one; never more than tiles
+  // 2.84 ms with one epilogue group, - / 2.66 / 2.61 / 2.64 ms with two);
+  // SSAM_CONV_ISSUERS=1..4 pins one; never more than tiles
   const char* ei = getenv("SSAM_CONV_ISSUERS");
-  int issuers = (ei && ei[0] >= '1' && ei[0] <= '4') ? ei[0] - '0' : 2;
+  int issuers = (ei && ei[0] >= '1' && ei[0] <= '4') ? ei[0] - '0' : 3;
   issuers = std::min(issuers, p.tiles);
   if (!zstack && !make_plan(n, dil, &p)) return SSAM_ERR_UNSUPPORTED;
   ConvArgs a;
@@ -698,10 +702,27 @@ int conv3d_ring(const void* in, const void* addend, const void* w, int ci_total,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimit));
     SSAM_CUDA_TRY(cudaFuncSetAttribute(conv3d_zstack_kernel<4>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimit));
+    SSAM_CUDA_TRY(cudaFuncSetAttribute(conv3d_zstack_kernel<2, 2>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimit));
+    SSAM_CUDA_TRY(cudaFuncSetAttribute(conv3d_zstack_kernel<3, 2>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimit));
+    SSAM_CUDA_TRY(cudaFuncSetAttribute(conv3d_zstack_kernel<4, 2>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemLimit));
     attr_set = true;
   }
   const int64_t grid = std::min<int64_t>(a.items, (int64_t)sms * p.ctas_per_sm);
-  if (zstack && issuers == 4)
+  // epilogue groups: 2 by default where there are two tiles to share
+  // (forward 2.89 -> 2.66 ms at two issuers); SSAM_CONV_EPI=1 keeps one
+  // (one-issuer kernels have one)
+  const char* ee = getenv("SSAM_CONV_EPI");
+  const int epi = (ee && ee[0] == '1') || p.tiles < 2 ? 1 : 2;
+  if (zstack && epi == 2 && issuers == 4)
+    conv3d_zstack_kernel<4, 2><<<(unsigned)grid, 32 * 13, p.smem, s>>>(a);
+  else if (zstack && epi == 2 && issuers == 3)
+    conv3d_zstack_kernel<3, 2><<<(unsigned)grid, 32 * 12, p.smem, s>>>(a);
+  else if (zstack && epi == 2 && issuers == 2)
+    conv3d_zstack_kernel<2, 2><<<(unsigned)grid, 32 * 11, p.smem, s>>>(a);
+  else if (zstack && issuers == 4)
     conv3d_zstack_kernel<4><<<(unsigned)grid, 32 * 9, p.smem, s>>>(a);
   else if (zstack && issuers == 3)
     conv3d_zstack_kernel<3><<<(unsigned)grid, 32 * 8, p.smem, s>>>(a);

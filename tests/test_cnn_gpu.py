@@ -224,20 +224,23 @@ def test_cnn_training_reduces_loss_and_roundtrips(cuda, tmp_path):
     other.close()
 
 
+@pytest.mark.parametrize("epi", [1, 2])
 @pytest.mark.parametrize("issuers", [1, 2, 3, 4])
 @pytest.mark.parametrize("ctas", [1, 2])
 @pytest.mark.parametrize("nsrc", [1, 2])
 @pytest.mark.parametrize("n", [128, 64, 32, 16])
-def test_zstack_kernel_equals_27_mma_kernel(cuda, monkeypatch, issuers, ctas, nsrc, n):
+def test_zstack_kernel_equals_27_mma_kernel(cuda, monkeypatch, epi, issuers, ctas, nsrc, n):
     """Dilation 1 runs the kernel that stacks the three z taps of an input
     plane on the MMA's N side (9 MMAs of N = 48 per plane and tile), with one
     or two CTAs a SM (SSAM_CONV_TWO_CTA=1: work items of fewer rows, 256 TMEM
     columns each); every output still sums its taps in the 27-MMA kernel's
     order, so all of them give the same bits (SSAM_CONV_RING27=1 selects the
     27-MMA kernel); likewise with 1 to 4 MMA-issuing warps a CTA
-    (SSAM_CONV_ISSUERS)."""
+    (SSAM_CONV_ISSUERS) and one or two groups of epilogue warps
+    (SSAM_CONV_EPI; two are compiled with 2-4 issuers)."""
     monkeypatch.setenv("SSAM_CONV_TWO_CTA", "1" if ctas == 2 else "0")
     monkeypatch.setenv("SSAM_CONV_ISSUERS", str(issuers))
+    monkeypatch.setenv("SSAM_CONV_EPI", str(epi))
     g = torch.Generator().manual_seed(7 * n + nsrc)
     nb = 2 if n <= 64 else 1
     xs = [torch.randn(nb, n, n, n, 16, generator=g).to(torch.bfloat16).to(cuda)
@@ -249,3 +252,4 @@ def test_zstack_kernel_equals_27_mma_kernel(cuda, monkeypatch, issuers, ctas, ns
     want = S.cnn_conv3d(*args, dilation=1, scale=0.75)
     S.device_status()
     assert torch.equal(got, want)
+
