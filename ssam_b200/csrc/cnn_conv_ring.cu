@@ -25,13 +25,16 @@
 // 128 per MMA tile; positions in the gaps or past the last row are computed
 // and discarded.
 //
-// Warp roles (one CTA per SM, persistent over items):
+// Warp roles of the 27-MMA kernel (one CTA per SM, persistent over items):
 //   warp 0      producer: 2 * (TY + 2d) row copies per plane into the ring
 //               (mbarrier full / empty per slot)
 //   warp 1      MMA issuer: TILES x 27 tcgen05.mma (128 x 16 x 16, BF16 in,
 //               FP32 in TMEM) per output plane; two accumulator buffers
 //   warps 2-5   epilogue: tcgen05.ld of each tile's accumulators, scale,
 //               add the optional addend, round to BF16, store valid voxels
+// Dilation 1 runs the z-stacked kernel further down instead (three z taps
+// on the MMA's N side; by default two CTAs a SM, three MMA-issuing warps
+// and two groups of epilogue warps a CTA).
 // Every wait is bounded by %globaltimer; on expiry the kernel records error
 // code 8 and winds down (drains its copies and MMAs, frees tensor memory).
 #include <stdlib.h>
